@@ -1,0 +1,346 @@
+"""B200-native blocked Bunch-Kaufman LDL^T.
+
+Python access to ``libbbk_b200.so`` (CUDA kernels for sm_100a behind the C ABI
+of ``include/bbk_ldlt.h``).  There is no CPU fallback: importing works without
+a GPU (so the library can be inspected), but every compute call needs the
+built library and an sm_100 device and raises otherwise.
+
+The class :class:`BlockLdltDecomposition` mirrors the reference's
+``naive_block_ldlt::BlockLdltDecomposition`` (include/block_ldlt_decomposition.h:
+11-31 in wentianshu/BlockedBunchKaufmanLDLT): construct from a symmetric
+matrix and a block size, ``factorize()``, then read the compact factors,
+permutation and pivot types, or ``reconstruct_original()`` in full mode.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libbbk_b200.so")
+
+BBK_OK = 0
+BBK_ERR_INVALID_ARGUMENT = 1
+BBK_ERR_OUT_OF_RANGE = 2
+BBK_ERR_LOGIC = 3
+BBK_ERR_ALLOC = 4
+BBK_ERR_CUDA = 5
+BBK_ERR_TIMEOUT = 6
+BBK_ERR_NO_DEVICE = 7
+BBK_ERR_WORKSPACE = 8
+
+UPDATE_FP64 = 0
+UPDATE_FP64_ORDERED = 1
+UPDATE_FP32 = 2
+UPDATE_MODES = {"fp64": UPDATE_FP64, "fp64_ordered": UPDATE_FP64_ORDERED, "fp32": UPDATE_FP32}
+
+# Every symbol include/bbk_ldlt.h declares.
+EXPORTS = (
+    "bbk_abi_version", "bbk_last_error", "bbk_status_string", "bbk_kernel_launch_count",
+    "bbk_set_wait_timeout_ns", "bbk_probe_bounded_wait", "bbk_factor_workspace_size",
+    "bbk_factor_device", "bbk_factor_device_async", "bbk_factor_host",
+    "bbk_solve_workspace_size", "bbk_solve_device", "bbk_solve_host", "bbk_factor_solve_host",
+    "bbk_reconstruct_device", "bbk_scale_one_by_one", "bbk_scale_two_by_two",
+    "bbk_update_trailing_block",
+)
+
+
+class BbkError(RuntimeError):
+    """A libbbk_b200 call failed; ``status`` is the bbk_status code."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"[{status}] {message}")
+        self.status = status
+
+
+class InvalidArgument(BbkError, ValueError):
+    """The reference's std::invalid_argument."""
+
+
+class OutOfRange(BbkError, IndexError):
+    """The reference's std::out_of_range."""
+
+
+class LogicError(BbkError):
+    """The reference's std::logic_error."""
+
+
+_EXC = {BBK_ERR_INVALID_ARGUMENT: InvalidArgument, BBK_ERR_OUT_OF_RANGE: OutOfRange,
+        BBK_ERR_LOGIC: LogicError}
+
+_c_int, _c_ll, _c_dbl, _c_sz, _vp = ctypes.c_int, ctypes.c_longlong, ctypes.c_double, ctypes.c_size_t, ctypes.c_void_p
+_lib = None
+
+
+def build(verbose: bool = False) -> str:
+    from . import buildlib as _b
+    return _b.build(verbose=verbose)
+
+
+def lib() -> ctypes.CDLL:
+    """Load libbbk_b200.so (raises if it was never built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with "
+                           "`python -c 'import __graft_entry__ as g; g.build()'`")
+    L = ctypes.CDLL(LIB_PATH)
+    sig = {
+        "bbk_abi_version": ([], _c_int),
+        "bbk_last_error": ([], ctypes.c_char_p),
+        "bbk_status_string": ([_c_int], ctypes.c_char_p),
+        "bbk_kernel_launch_count": ([], ctypes.c_ulonglong),
+        "bbk_set_wait_timeout_ns": ([ctypes.c_ulonglong], _c_int),
+        "bbk_probe_bounded_wait": ([_c_int, ctypes.c_ulonglong, _vp], _c_int),
+        "bbk_factor_workspace_size": ([_c_int, _c_int], _c_sz),
+        "bbk_factor_device": ([_c_int, _c_int, _vp, _c_ll, _vp, _vp, _vp, _c_int, _vp, _c_sz, _vp], _c_int),
+        "bbk_factor_device_async": ([_c_int, _c_int, _vp, _c_ll, _vp, _vp, _vp, _c_int, _vp, _c_sz,
+                                     _vp, _vp], _c_int),
+        "bbk_factor_host": ([_c_int, _c_int, _vp, _c_ll, _vp, _vp, _vp, _c_int], _c_int),
+        "bbk_solve_workspace_size": ([_c_int, _c_int], _c_sz),
+        "bbk_solve_device": ([_c_int, _vp, _c_ll, _vp, _vp, _c_int, _vp, _c_ll, _vp, _c_sz, _vp], _c_int),
+        "bbk_solve_host": ([_c_int, _vp, _c_ll, _vp, _vp, _c_int, _vp, _c_ll], _c_int),
+        "bbk_factor_solve_host": ([_c_int, _c_int, _vp, _c_ll, _vp, _vp, _vp, _c_int, _vp, _c_ll,
+                                   _c_int], _c_int),
+        "bbk_reconstruct_device": ([_c_int, _vp, _c_ll, _vp, _vp, _vp, _c_ll, _vp], _c_int),
+        "bbk_scale_one_by_one": ([_c_int, _c_dbl, _vp, _c_int, _vp, _c_int, _vp], _c_int),
+        "bbk_scale_two_by_two": ([_c_int, _c_dbl, _c_dbl, _c_dbl, _vp, _c_int, _vp, _c_int, _vp,
+                                  _c_int, _vp, _c_int, _vp], _c_int),
+        "bbk_update_trailing_block": ([_c_int, _c_int, _c_int, _vp, _c_int, _vp, _c_int, _vp,
+                                       _c_int, _c_int, _vp], _c_int),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = L
+    return L
+
+
+def check(status: int) -> None:
+    if status != BBK_OK:
+        msg = lib().bbk_last_error().decode(errors="replace")
+        raise _EXC.get(status, BbkError)(status, msg)
+
+
+def kernel_launch_count() -> int:
+    return int(lib().bbk_kernel_launch_count())
+
+
+def set_wait_timeout_ns(ns: int) -> None:
+    check(lib().bbk_set_wait_timeout_ns(int(ns)))
+
+
+def _np_ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _mode(mode) -> int:
+    if isinstance(mode, str):
+        return UPDATE_MODES[mode]
+    return int(mode)
+
+
+# ---------------------------------------------------------------------------
+# Device (torch CUDA tensor) entry points
+# ---------------------------------------------------------------------------
+def _stream_ptr(stream):
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def factor_device(a, block_size: int, mode="fp64", stream=None, workspace=None,
+                  sync: bool = True):
+    """Factor the upper triangle of the CUDA float64 tensor ``a`` (n x lda,
+    row-major, modified in place into compact factors).  Returns device int32
+    tensors (perm, pivot_types, panel_end)."""
+    import torch
+    if a.dtype != torch.float64 or not a.is_cuda or a.dim() != 2 or a.stride(1) != 1:
+        raise InvalidArgument(BBK_ERR_INVALID_ARGUMENT, "need a row-major CUDA float64 matrix")
+    n = a.shape[0]
+    nb = (n + block_size - 1) // block_size if block_size > 0 else 0
+    perm = torch.empty(n, dtype=torch.int32, device=a.device)
+    pt = torch.empty(n, dtype=torch.int32, device=a.device)
+    pe = torch.empty(max(nb, 1), dtype=torch.int32, device=a.device)
+    ws_ptr, ws_bytes = (None, 0)
+    if workspace is not None:
+        ws_ptr, ws_bytes = ctypes.c_void_p(workspace.data_ptr()), workspace.numel() * workspace.element_size()
+    if sync:
+        check(lib().bbk_factor_device(n, block_size, ctypes.c_void_p(a.data_ptr()), a.stride(0),
+                                      ctypes.c_void_p(perm.data_ptr()), ctypes.c_void_p(pt.data_ptr()),
+                                      ctypes.c_void_p(pe.data_ptr()), _mode(mode), ws_ptr, ws_bytes,
+                                      _stream_ptr(stream)))
+    else:
+        status = torch.zeros(1, dtype=torch.int32, device=a.device)
+        check(lib().bbk_factor_device_async(n, block_size, ctypes.c_void_p(a.data_ptr()), a.stride(0),
+                                            ctypes.c_void_p(perm.data_ptr()),
+                                            ctypes.c_void_p(pt.data_ptr()),
+                                            ctypes.c_void_p(pe.data_ptr()), _mode(mode), ws_ptr,
+                                            ws_bytes, ctypes.c_void_p(status.data_ptr()),
+                                            _stream_ptr(stream)))
+        return perm, pt, pe, status
+    return perm, pt, pe
+
+
+def factor_workspace_size(n: int, block_size: int) -> int:
+    return int(lib().bbk_factor_workspace_size(n, block_size))
+
+
+def solve_workspace_size(n: int, nrhs: int) -> int:
+    return int(lib().bbk_solve_workspace_size(n, nrhs))
+
+
+def solve_device(f, perm, pivot_types, b, stream=None, workspace=None):
+    """Solve with compact factors on the device.  ``b`` is a CUDA float64
+    tensor of shape (nrhs, n) (each row one right-hand side), overwritten."""
+    n = f.shape[0]
+    nrhs = b.shape[0] if b.dim() == 2 else 1
+    ldb = b.stride(0) if b.dim() == 2 else n
+    ws_ptr, ws_bytes = (None, 0)
+    if workspace is not None:
+        ws_ptr, ws_bytes = ctypes.c_void_p(workspace.data_ptr()), workspace.numel() * workspace.element_size()
+    check(lib().bbk_solve_device(n, ctypes.c_void_p(f.data_ptr()), f.stride(0),
+                                 ctypes.c_void_p(perm.data_ptr()), ctypes.c_void_p(pivot_types.data_ptr()),
+                                 nrhs, ctypes.c_void_p(b.data_ptr()), ldb, ws_ptr, ws_bytes,
+                                 _stream_ptr(stream)))
+    return b
+
+
+def reconstruct_device(f, perm, pivot_types, stream=None):
+    import torch
+    n = f.shape[0]
+    out = torch.empty((n, n), dtype=torch.float64, device=f.device)
+    check(lib().bbk_reconstruct_device(n, ctypes.c_void_p(f.data_ptr()), f.stride(0),
+                                       ctypes.c_void_p(perm.data_ptr()),
+                                       ctypes.c_void_p(pivot_types.data_ptr()),
+                                       ctypes.c_void_p(out.data_ptr()), n, _stream_ptr(stream)))
+    return out
+
+
+def probe_bounded_wait(ctas: int, timeout_ns: int, stream=None) -> int:
+    """Run the bounded-wait probe; returns the bbk_status (BBK_ERR_TIMEOUT
+    when the device-side wait bound works)."""
+    return int(lib().bbk_probe_bounded_wait(ctas, timeout_ns, _stream_ptr(stream)))
+
+
+# ---------------------------------------------------------------------------
+# Host (numpy) entry points
+# ---------------------------------------------------------------------------
+@dataclass
+class HostFactors:
+    factors: np.ndarray
+    perm: np.ndarray
+    pivot_types: np.ndarray
+    panel_end: np.ndarray
+
+
+def factor_host(a: np.ndarray, block_size: int, mode="fp64") -> HostFactors:
+    """Factor on the GPU from host memory; ``a`` is not modified."""
+    f = np.array(a, dtype=np.float64, order="C", copy=True)
+    n = f.shape[0]
+    nb = (n + block_size - 1) // block_size if block_size > 0 else 1
+    perm = np.zeros(n, np.int32)
+    pt = np.zeros(n, np.int32)
+    pe = np.zeros(max(nb, 1), np.int32)
+    check(lib().bbk_factor_host(n, block_size, _np_ptr(f), f.shape[1], _np_ptr(perm), _np_ptr(pt),
+                                _np_ptr(pe), _mode(mode)))
+    return HostFactors(f, perm, pt, pe)
+
+
+def factor_solve_host(a: np.ndarray, block_size: int, b: np.ndarray, mode="fp64"):
+    """One call: factor ``a`` and solve for the columns of ``b`` (n or n x nrhs)."""
+    f = np.array(a, dtype=np.float64, order="C", copy=True)
+    n = f.shape[0]
+    bb = np.array(b, dtype=np.float64, copy=True)
+    one = bb.ndim == 1
+    bt = np.ascontiguousarray(bb.reshape(n, -1).T)  # (nrhs, n): each row one rhs
+    nb = (n + block_size - 1) // block_size if block_size > 0 else 1
+    perm = np.zeros(n, np.int32)
+    pt = np.zeros(n, np.int32)
+    pe = np.zeros(max(nb, 1), np.int32)
+    check(lib().bbk_factor_solve_host(n, block_size, _np_ptr(f), f.shape[1], _np_ptr(perm),
+                                      _np_ptr(pt), _np_ptr(pe), bt.shape[0], _np_ptr(bt), n,
+                                      _mode(mode)))
+    x = bt.T.copy()
+    return HostFactors(f, perm, pt, pe), (x[:, 0] if one else x)
+
+
+def solve_host(fac: HostFactors, b: np.ndarray) -> np.ndarray:
+    n = fac.factors.shape[0]
+    bb = np.array(b, dtype=np.float64, copy=True)
+    one = bb.ndim == 1
+    bt = np.ascontiguousarray(bb.reshape(n, -1).T)
+    ff = np.ascontiguousarray(fac.factors)
+    check(lib().bbk_solve_host(n, _np_ptr(ff), ff.shape[1], _np_ptr(fac.perm),
+                               _np_ptr(fac.pivot_types), bt.shape[0], _np_ptr(bt), n))
+    x = bt.T.copy()
+    return x[:, 0] if one else x
+
+
+# ---------------------------------------------------------------------------
+# Mirror of the reference's BlockLdltDecomposition
+# ---------------------------------------------------------------------------
+class BlockLdltDecomposition:
+    """Python mirror of naive_block_ldlt::BlockLdltDecomposition.
+
+    ``matrix`` is a dense symmetric matrix (only the upper triangle is read,
+    like BlockMatrix(RegularMatrix, block_size, MatrixTriangle::kUpper)) and
+    ``block_size`` the BlockMatrix block size.  ``full=True`` is kFull mode
+    (L/D factors and reconstruct_original available), ``full=False`` is
+    kCompactOnly.  The factorization runs on the GPU; nothing runs on the CPU.
+    """
+
+    def __init__(self, matrix: np.ndarray, block_size: int, full: bool = True,
+                 mode="fp64", lower: bool = False):
+        m = np.asarray(matrix, dtype=np.float64)
+        if m.ndim != 2 or m.shape[0] != m.shape[1]:
+            raise InvalidArgument(BBK_ERR_INVALID_ARGUMENT, "block matrix input must be square")
+        if m.shape[0] <= 0:
+            raise InvalidArgument(BBK_ERR_INVALID_ARGUMENT, "matrix size must be positive")
+        if block_size <= 0:
+            raise InvalidArgument(BBK_ERR_INVALID_ARGUMENT, "block size must be positive")
+        self._input = np.ascontiguousarray(m.T if lower else m)
+        self.block_size = block_size
+        self.full = full
+        self.mode = mode
+        self._fac: HostFactors | None = None
+
+    def factorize(self) -> None:
+        self._fac = factor_host(self._input, self.block_size, self.mode)
+
+    def _need(self) -> HostFactors:
+        if self._fac is None:
+            raise LogicError(BBK_ERR_LOGIC, "Factorize() must be called first")
+        return self._fac
+
+    def compact_factors(self) -> np.ndarray:
+        """Upper triangle of the compact factor (lower triangle zero)."""
+        return np.triu(self._need().factors)
+
+    def permutation(self) -> np.ndarray:
+        return self._need().perm
+
+    def pivot_types(self) -> np.ndarray:
+        return self._need().pivot_types
+
+    def panel_end(self) -> np.ndarray:
+        return self._need().panel_end
+
+    def reconstruct_original(self) -> np.ndarray:
+        if not self.full:
+            raise LogicError(BBK_ERR_LOGIC, "ReconstructOriginal() requires full factor storage")
+        fac = self._need()
+        import torch
+        dev = torch.device("cuda")
+        f = torch.from_numpy(np.ascontiguousarray(fac.factors)).to(dev)
+        perm = torch.from_numpy(fac.perm).to(dev)
+        pt = torch.from_numpy(fac.pivot_types).to(dev)
+        return reconstruct_device(f, perm, pt).cpu().numpy()
+
+    def solve(self, b: np.ndarray) -> np.ndarray:
+        return solve_host(self._need(), b)

@@ -1,0 +1,149 @@
+// Internal declarations shared by the CUDA translation units of libbbk_b200.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstddef>
+
+#include "bbk_ldlt.h"
+
+namespace bbk {
+
+// ---------------------------------------------------------------------------
+// Host-side helpers (capi.cu)
+// ---------------------------------------------------------------------------
+int set_error(int status, const char* fmt, ...);
+int cuda_error(cudaError_t err, const char* what);
+void count_launch(unsigned n = 1);
+unsigned long long wait_timeout_ns();
+int device_sm_count();
+
+#define BBK_CUDA_TRY(expr)                                            \
+  do {                                                                \
+    cudaError_t bbk_err_ = (expr);                                    \
+    if (bbk_err_ != cudaSuccess) return ::bbk::cuda_error(bbk_err_, #expr); \
+  } while (0)
+
+inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+// Bunch-Kaufman threshold (1 + sqrt(17)) / 8, the reference's literal
+// (src/block_ldlt_decomposition.cc:14).
+constexpr double kAlpha = 0.6403882032022076;
+constexpr double kDblEpsilon = 2.220446049250313080847e-16;  // DBL_EPSILON
+
+// ---------------------------------------------------------------------------
+// Device helpers
+// ---------------------------------------------------------------------------
+// Exactly-rounded arithmetic that the compiler may not contract into FMAs:
+// the panel reproduces the reference's operation order bit for bit.
+__device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double xadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double xsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double xdiv(double a, double b) { return __ddiv_rn(a, b); }
+
+// L2-coherent load (bypasses L1): data written by other CTAs of the same
+// grid is read through these after an exchange.
+__device__ __forceinline__ double ldcg(const double* p) { return __ldcg(p); }
+__device__ __forceinline__ int ldcg(const int* p) { return __ldcg(p); }
+
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ int ld_relaxed_s32(const int* p) {
+  int v;
+  asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void fence_acq_rel_gpu() {
+  asm volatile("fence.acq_rel.gpu;" ::: "memory");
+}
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Device status words shared by every kernel of one factorization.
+struct DeviceState {
+  int kstart[2];  // first row of panel P is kstart[P & 1]; panel P writes
+                  // its end (= start of P + 1) into kstart[(P + 1) & 1]
+  int abort;      // nonzero: a kernel gave up; every later kernel returns
+  int status;     // bbk_status of the factorization
+};
+
+// ---------------------------------------------------------------------------
+// Tagged-slot exchange: a grid-wide barrier fused with an all-gather of one
+// small record per CTA.  Every 64-bit word carries the exchange's 32-bit tag
+// in its high half, so a reader knows a word is current without any other
+// ordering; the writer's release fence before its stores and the reader's
+// acquire fence after seeing all tags order everything else.  Two slot sets
+// alternate (tag parity): no CTA can be two exchanges ahead of another.
+// ---------------------------------------------------------------------------
+constexpr int kSlotWords = 16;   // words per CTA record
+constexpr int kMaxPub = 6;       // published doubles per record
+
+__device__ __forceinline__ unsigned long long tag_word(unsigned tag, unsigned v) {
+  return (static_cast<unsigned long long>(tag) << 32) | v;
+}
+
+}  // namespace bbk
+
+// Launch entry points implemented in the .cu files (host side).
+namespace bbk {
+struct FactorPlan;
+int panel_grid_size(int n);
+int launch_init(int n, int* perm, int* pivot_types, DeviceState* st,
+                unsigned long long* slots, size_t slot_words, cudaStream_t s);
+int launch_panel(const FactorPlan& plan, int panel, cudaStream_t s);
+int launch_finalize(const FactorPlan& plan, int panel, cudaStream_t s);
+int launch_update(const FactorPlan& plan, int panel, cudaStream_t s);
+int launch_status_copy(const DeviceState* st, int* status_out, cudaStream_t s);
+int launch_probe_wait(int ctas, unsigned long long timeout_ns, DeviceState* st,
+                      unsigned long long* slots, cudaStream_t s);
+int launch_update_block(int rows, int cols, int inner, const double* left, int ls,
+                        const double* ws, int wss, double* target, int ts, int mode,
+                        cudaStream_t s);
+int launch_scale_1x1(int count, double pivot, const double* src, int ss, double* dst,
+                     int ds, cudaStream_t s);
+int launch_scale_2x2(int count, double a, double b, double c, const double* s1, int s1s,
+                     const double* s2, int s2s, double* d1, int d1s, double* d2, int d2s,
+                     cudaStream_t s);
+int solve_enqueue(int n, const double* f, long long ldf, const int* perm,
+                  const int* pivot_types, int nrhs, double* b, long long ldb,
+                  double* work, cudaStream_t s);
+size_t solve_work_doubles(int n, int nrhs);
+int reconstruct_enqueue(int n, const double* f, long long ldf, const int* perm,
+                        const int* pivot_types, double* out, long long ldo,
+                        double* work, cudaStream_t s);
+
+// Everything a factorization's kernels need: the caller's matrix and the
+// carved-up workspace.
+struct FactorPlan {
+  int n = 0;
+  int b = 0;           // reference block size (nominal panel width)
+  int nb = 0;          // number of panels
+  int mode = 0;        // bbk_update_mode
+  double* a = nullptr;
+  long long lda = 0;
+  int* perm = nullptr;
+  int* pivot_types = nullptr;
+  int* panel_end = nullptr;  // may be null
+  // workspace
+  double* w = nullptr;       // (b+1) rows x ldw: the panel's W rows
+  long long ldw = 0;
+  double* ucm = nullptr;     // n x ldu column-major copy of the panel's U rows
+  int ldu = 0;
+  double* uout = nullptr;    // (b+1) x ldu: final columns of the panel's pivots
+  double* wc = nullptr;      // n: candidate column
+  unsigned long long* slots = nullptr;  // 2 x grid x kSlotWords
+  DeviceState* state = nullptr;
+  int grid = 0;              // CTAs of the panel kernel
+  unsigned long long timeout_ns = 0;
+};
+}  // namespace bbk

@@ -1,0 +1,474 @@
+// extern "C" entry points of libbbk_b200 (declared in include/bbk_ldlt.h).
+#include <atomic>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+
+#include "bbk_internal.cuh"
+
+namespace bbk {
+namespace {
+
+thread_local char g_error[1024] = "";
+std::atomic<unsigned long long> g_launches{0};
+std::atomic<unsigned long long> g_timeout_ns{5000000000ull};
+
+constexpr int kMaxPanelGrid = 1024;
+constexpr size_t kAlign = 256;
+
+int g_sm_count[64] = {0};
+
+int check_device() {
+  int dev = 0;
+  cudaError_t err = cudaGetDevice(&dev);
+  if (err != cudaSuccess) return set_error(BBK_ERR_NO_DEVICE, "no CUDA device: %s", cudaGetErrorString(err));
+  int major = 0;
+  err = cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+  if (err != cudaSuccess) return cuda_error(err, "cudaDeviceGetAttribute");
+  if (major != 10)
+    return set_error(BBK_ERR_NO_DEVICE,
+                     "libbbk_b200 is built for sm_100a only; device %d is sm_%d0", dev, major);
+  return BBK_OK;
+}
+
+struct Carver {
+  char* base;
+  size_t off = 0;
+  template <typename T>
+  T* take(size_t count) {
+    T* p = reinterpret_cast<T*>(base ? base + off : nullptr);
+    off = align_up(off + count * sizeof(T), kAlign);
+    return p;
+  }
+};
+
+// Lays out (or, with base == nullptr, measures) the factorization workspace.
+size_t carve_factor(FactorPlan& plan, char* base) {
+  const int n = plan.n, b = plan.b;
+  const long long npad = static_cast<long long>(align_up(static_cast<size_t>(n), 64));
+  plan.ldw = npad;
+  plan.ldu = static_cast<int>(align_up(static_cast<size_t>(b) + 2, 4));
+  Carver c{base};
+  plan.state = c.take<DeviceState>(1);
+  plan.slots = c.take<unsigned long long>(2ull * kMaxPanelGrid * kSlotWords);
+  plan.w = c.take<double>(static_cast<size_t>(b + 2) * npad);
+  plan.ucm = c.take<double>(static_cast<size_t>(npad) * plan.ldu);
+  plan.uout = c.take<double>(static_cast<size_t>(b + 2) * plan.ldu);
+  plan.wc = c.take<double>(static_cast<size_t>(npad));
+  c.take<int>(4);  // status word for the synchronous entry point
+  return c.off;
+}
+
+int validate_factor_args(int n, int block_size, const double* a, long long lda, const int* perm,
+                         const int* pivot_types, int mode) {
+  if (n <= 0) return set_error(BBK_ERR_INVALID_ARGUMENT, "matrix size must be positive");
+  if (block_size <= 0) return set_error(BBK_ERR_INVALID_ARGUMENT, "block size must be positive");
+  if (lda < n) return set_error(BBK_ERR_INVALID_ARGUMENT, "lda (%lld) < n (%d)", lda, n);
+  if (!a || !perm || !pivot_types)
+    return set_error(BBK_ERR_INVALID_ARGUMENT, "null matrix, permutation or pivot array");
+  if (mode != BBK_UPDATE_FP64 && mode != BBK_UPDATE_FP64_ORDERED && mode != BBK_UPDATE_FP32)
+    return set_error(BBK_ERR_INVALID_ARGUMENT, "unknown update mode %d", mode);
+  return BBK_OK;
+}
+
+}  // namespace
+
+int set_error(int status, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_error, sizeof(g_error), fmt, ap);
+  va_end(ap);
+  return status;
+}
+
+int cuda_error(cudaError_t err, const char* what) {
+  snprintf(g_error, sizeof(g_error), "%s: %s", what, cudaGetErrorString(err));
+  return err == cudaErrorMemoryAllocation ? BBK_ERR_ALLOC : BBK_ERR_CUDA;
+}
+
+void count_launch(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+unsigned long long wait_timeout_ns() { return g_timeout_ns.load(std::memory_order_relaxed); }
+
+int device_sm_count() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (g_sm_count[dev] == 0) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0)
+      v = 148;
+    g_sm_count[dev] = v;
+  }
+  return g_sm_count[dev];
+}
+
+// Enqueue a whole factorization for an already carved plan.
+static int enqueue_factor(FactorPlan& plan, int* status_device, cudaStream_t s) {
+  int rc = launch_init(plan.n, plan.perm, plan.pivot_types, plan.state, plan.slots,
+                       2ull * kMaxPanelGrid * kSlotWords, s);
+  if (rc) return rc;
+  for (int panel = 0; panel < plan.nb; ++panel) {
+    if ((rc = launch_panel(plan, panel, s))) return rc;
+    if ((rc = launch_finalize(plan, panel, s))) return rc;
+    if ((rc = launch_update(plan, panel, s))) return rc;
+  }
+  return launch_status_copy(plan.state, status_device, s);
+}
+
+}  // namespace bbk
+
+using namespace bbk;
+
+extern "C" {
+
+int bbk_abi_version(void) { return BBK_ABI_VERSION; }
+
+const char* bbk_last_error(void) { return g_error; }
+
+const char* bbk_status_string(int status) {
+  switch (status) {
+    case BBK_OK: return "ok";
+    case BBK_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case BBK_ERR_OUT_OF_RANGE: return "out of range";
+    case BBK_ERR_LOGIC: return "logic error";
+    case BBK_ERR_ALLOC: return "allocation failed";
+    case BBK_ERR_CUDA: return "CUDA error";
+    case BBK_ERR_TIMEOUT: return "device-side wait timed out";
+    case BBK_ERR_NO_DEVICE: return "no usable sm_100 device";
+    case BBK_ERR_WORKSPACE: return "workspace too small";
+    default: return "unknown status";
+  }
+}
+
+unsigned long long bbk_kernel_launch_count(void) {
+  return g_launches.load(std::memory_order_relaxed);
+}
+
+int bbk_set_wait_timeout_ns(unsigned long long timeout_ns) {
+  if (timeout_ns == 0) return set_error(BBK_ERR_INVALID_ARGUMENT, "timeout must be positive");
+  g_timeout_ns.store(timeout_ns, std::memory_order_relaxed);
+  return BBK_OK;
+}
+
+size_t bbk_factor_workspace_size(int n, int block_size) {
+  if (n <= 0 || block_size <= 0) return 0;
+  FactorPlan plan;
+  plan.n = n;
+  plan.b = block_size;
+  return carve_factor(plan, nullptr);
+}
+
+int bbk_factor_device_async(int n, int block_size, double* a, long long lda, int* perm,
+                            int* pivot_types, int* panel_end, int update_mode, void* workspace,
+                            size_t workspace_bytes, int* status_device, void* stream) {
+  int rc = validate_factor_args(n, block_size, a, lda, perm, pivot_types, update_mode);
+  if (rc) return rc;
+  if ((rc = check_device())) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  FactorPlan plan;
+  plan.n = n;
+  plan.b = block_size;
+  plan.nb = (n + block_size - 1) / block_size;
+  plan.mode = update_mode;
+  plan.a = a;
+  plan.lda = lda;
+  plan.perm = perm;
+  plan.pivot_types = pivot_types;
+  plan.panel_end = panel_end;
+  plan.grid = panel_grid_size(n);
+  plan.timeout_ns = wait_timeout_ns();
+  const size_t need = carve_factor(plan, nullptr);
+  char* base = static_cast<char*>(workspace);
+  bool owned = false;
+  if (base == nullptr) {
+    BBK_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&base), need, s));
+    owned = true;
+  } else if (workspace_bytes < need) {
+    return set_error(BBK_ERR_WORKSPACE, "factor workspace needs %zu bytes, got %zu", need,
+                     workspace_bytes);
+  }
+  carve_factor(plan, base);
+  int* status = status_device;
+  if (status == nullptr) {
+    Carver c{base};
+    c.off = need - kAlign;
+    status = c.take<int>(1);
+  }
+  rc = enqueue_factor(plan, status, s);
+  if (owned) {
+    cudaError_t err = cudaFreeAsync(base, s);
+    if (!rc && err != cudaSuccess) rc = cuda_error(err, "cudaFreeAsync");
+  }
+  return rc;
+}
+
+int bbk_factor_device(int n, int block_size, double* a, long long lda, int* perm,
+                      int* pivot_types, int* panel_end, int update_mode, void* workspace,
+                      size_t workspace_bytes, void* stream) {
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int* d_status = nullptr;
+  int rc = validate_factor_args(n, block_size, a, lda, perm, pivot_types, update_mode);
+  if (rc) return rc;
+  if ((rc = check_device())) return rc;
+  BBK_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&d_status), sizeof(int), s));
+  rc = bbk_factor_device_async(n, block_size, a, lda, perm, pivot_types, panel_end, update_mode,
+                               workspace, workspace_bytes, d_status, s);
+  int h_status = BBK_OK;
+  if (!rc) {
+    cudaError_t err = cudaMemcpyAsync(&h_status, d_status, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+    if (err != cudaSuccess) rc = cuda_error(err, "factorization");
+  }
+  cudaFreeAsync(d_status, s);
+  if (rc) return rc;
+  if (h_status != BBK_OK)
+    return set_error(h_status, "factorization aborted on the device: %s", bbk_status_string(h_status));
+  return BBK_OK;
+}
+
+int bbk_factor_host(int n, int block_size, double* a, long long lda, int* perm, int* pivot_types,
+                    int* panel_end, int update_mode) {
+  return bbk_factor_solve_host(n, block_size, a, lda, perm, pivot_types, panel_end, 0, nullptr, 0,
+                               update_mode);
+}
+
+size_t bbk_solve_workspace_size(int n, int nrhs) {
+  if (n <= 0 || nrhs <= 0) return 0;
+  return solve_work_doubles(n, nrhs) * sizeof(double);
+}
+
+static int validate_solve(int n, const double* f, long long ldf, const int* perm, const int* pt,
+                          int nrhs, const double* b, long long ldb) {
+  if (n <= 0) return set_error(BBK_ERR_INVALID_ARGUMENT, "matrix size must be positive");
+  if (nrhs < 0) return set_error(BBK_ERR_INVALID_ARGUMENT, "nrhs must be non-negative");
+  if (ldf < n || (nrhs > 0 && ldb < n))
+    return set_error(BBK_ERR_INVALID_ARGUMENT, "leading dimension smaller than n");
+  if (!f || !perm || !pt || (nrhs > 0 && !b))
+    return set_error(BBK_ERR_INVALID_ARGUMENT, "null factor, permutation, pivot or rhs array");
+  return BBK_OK;
+}
+
+int bbk_solve_device(int n, const double* factors, long long ldf, const int* perm,
+                     const int* pivot_types, int nrhs, double* b, long long ldb, void* workspace,
+                     size_t workspace_bytes, void* stream) {
+  int rc = validate_solve(n, factors, ldf, perm, pivot_types, nrhs, b, ldb);
+  if (rc) return rc;
+  if (nrhs == 0) return BBK_OK;
+  if ((rc = check_device())) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const size_t need = bbk_solve_workspace_size(n, nrhs);
+  double* work = static_cast<double*>(workspace);
+  bool owned = false;
+  if (work == nullptr) {
+    BBK_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&work), need, s));
+    owned = true;
+  } else if (workspace_bytes < need) {
+    return set_error(BBK_ERR_WORKSPACE, "solve workspace needs %zu bytes, got %zu", need,
+                     workspace_bytes);
+  }
+  rc = solve_enqueue(n, factors, ldf, perm, pivot_types, nrhs, b, ldb, work, s);
+  if (owned) cudaFreeAsync(work, s);
+  if (rc) return rc;
+  BBK_CUDA_TRY(cudaStreamSynchronize(s));
+  return BBK_OK;
+}
+
+int bbk_solve_host(int n, const double* factors, long long ldf, const int* perm,
+                   const int* pivot_types, int nrhs, double* b, long long ldb) {
+  int rc = validate_solve(n, factors, ldf, perm, pivot_types, nrhs, b, ldb);
+  if (rc) return rc;
+  if (nrhs == 0) return BBK_OK;
+  if ((rc = check_device())) return rc;
+  cudaStream_t s;
+  BBK_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  double *d_f = nullptr, *d_b = nullptr, *work = nullptr;
+  int *d_perm = nullptr, *d_pt = nullptr;
+  const size_t fbytes = static_cast<size_t>(n) * ldf * sizeof(double);
+  const size_t bbytes = static_cast<size_t>(nrhs) * ldb * sizeof(double);
+  cudaError_t err = cudaMallocAsync(reinterpret_cast<void**>(&d_f), fbytes, s);
+  if (err == cudaSuccess) err = cudaMallocAsync(reinterpret_cast<void**>(&d_b), bbytes, s);
+  if (err == cudaSuccess) err = cudaMallocAsync(reinterpret_cast<void**>(&d_perm), n * sizeof(int), s);
+  if (err == cudaSuccess) err = cudaMallocAsync(reinterpret_cast<void**>(&d_pt), n * sizeof(int), s);
+  if (err == cudaSuccess)
+    err = cudaMallocAsync(reinterpret_cast<void**>(&work), bbk_solve_workspace_size(n, nrhs), s);
+  if (err == cudaSuccess) err = cudaMemcpyAsync(d_f, factors, fbytes, cudaMemcpyHostToDevice, s);
+  if (err == cudaSuccess) err = cudaMemcpyAsync(d_b, b, bbytes, cudaMemcpyHostToDevice, s);
+  if (err == cudaSuccess) err = cudaMemcpyAsync(d_perm, perm, n * sizeof(int), cudaMemcpyHostToDevice, s);
+  if (err == cudaSuccess) err = cudaMemcpyAsync(d_pt, pivot_types, n * sizeof(int), cudaMemcpyHostToDevice, s);
+  if (err != cudaSuccess) {
+    rc = cuda_error(err, "solve setup");
+  } else {
+    rc = solve_enqueue(n, d_f, ldf, d_perm, d_pt, nrhs, d_b, ldb, work, s);
+    if (!rc) {
+      err = cudaMemcpyAsync(b, d_b, bbytes, cudaMemcpyDeviceToHost, s);
+      if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+      if (err != cudaSuccess) rc = cuda_error(err, "solve");
+    }
+  }
+  cudaFreeAsync(d_f, s);
+  cudaFreeAsync(d_b, s);
+  cudaFreeAsync(d_perm, s);
+  cudaFreeAsync(d_pt, s);
+  cudaFreeAsync(work, s);
+  cudaStreamSynchronize(s);
+  cudaStreamDestroy(s);
+  return rc;
+}
+
+int bbk_factor_solve_host(int n, int block_size, double* a, long long lda, int* perm,
+                          int* pivot_types, int* panel_end, int nrhs, double* b, long long ldb,
+                          int update_mode) {
+  int rc = validate_factor_args(n, block_size, a, lda, perm, pivot_types, update_mode);
+  if (rc) return rc;
+  if (nrhs < 0 || (nrhs > 0 && (!b || ldb < n)))
+    return set_error(BBK_ERR_INVALID_ARGUMENT, "bad right-hand side arguments");
+  if ((rc = check_device())) return rc;
+  cudaStream_t s;
+  BBK_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  const int nb = (n + block_size - 1) / block_size;
+  const size_t abytes = static_cast<size_t>(n) * lda * sizeof(double);
+  const size_t bbytes = static_cast<size_t>(nrhs) * ldb * sizeof(double);
+  const size_t fws = bbk_factor_workspace_size(n, block_size);
+  const size_t sws = nrhs > 0 ? bbk_solve_workspace_size(n, nrhs) : 0;
+  double *d_a = nullptr, *d_b = nullptr;
+  int *d_perm = nullptr, *d_pt = nullptr, *d_pe = nullptr, *d_status = nullptr;
+  char* ws = nullptr;
+  int h_status = BBK_OK;
+  cudaError_t err = cudaMallocAsync(reinterpret_cast<void**>(&d_a), abytes, s);
+  if (err == cudaSuccess && nrhs > 0) err = cudaMallocAsync(reinterpret_cast<void**>(&d_b), bbytes, s);
+  if (err == cudaSuccess) err = cudaMallocAsync(reinterpret_cast<void**>(&d_perm), n * sizeof(int), s);
+  if (err == cudaSuccess) err = cudaMallocAsync(reinterpret_cast<void**>(&d_pt), n * sizeof(int), s);
+  if (err == cudaSuccess) err = cudaMallocAsync(reinterpret_cast<void**>(&d_pe), nb * sizeof(int), s);
+  if (err == cudaSuccess) err = cudaMallocAsync(reinterpret_cast<void**>(&d_status), sizeof(int), s);
+  if (err == cudaSuccess)
+    err = cudaMallocAsync(reinterpret_cast<void**>(&ws), fws > sws ? fws : sws, s);
+  if (err == cudaSuccess) err = cudaMemcpyAsync(d_a, a, abytes, cudaMemcpyHostToDevice, s);
+  if (err == cudaSuccess && nrhs > 0) err = cudaMemcpyAsync(d_b, b, bbytes, cudaMemcpyHostToDevice, s);
+  if (err != cudaSuccess) {
+    rc = cuda_error(err, "factorization setup");
+  } else {
+    rc = bbk_factor_device_async(n, block_size, d_a, lda, d_perm, d_pt, d_pe, update_mode, ws, fws,
+                                 d_status, s);
+    if (!rc && nrhs > 0) rc = solve_enqueue(n, d_a, lda, d_perm, d_pt, nrhs, d_b, ldb,
+                                            reinterpret_cast<double*>(ws), s);
+    if (!rc) {
+      err = cudaMemcpyAsync(a, d_a, abytes, cudaMemcpyDeviceToHost, s);
+      if (err == cudaSuccess) err = cudaMemcpyAsync(perm, d_perm, n * sizeof(int), cudaMemcpyDeviceToHost, s);
+      if (err == cudaSuccess) err = cudaMemcpyAsync(pivot_types, d_pt, n * sizeof(int), cudaMemcpyDeviceToHost, s);
+      if (err == cudaSuccess && panel_end)
+        err = cudaMemcpyAsync(panel_end, d_pe, nb * sizeof(int), cudaMemcpyDeviceToHost, s);
+      if (err == cudaSuccess && nrhs > 0) err = cudaMemcpyAsync(b, d_b, bbytes, cudaMemcpyDeviceToHost, s);
+      if (err == cudaSuccess) err = cudaMemcpyAsync(&h_status, d_status, sizeof(int), cudaMemcpyDeviceToHost, s);
+      if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+      if (err != cudaSuccess) rc = cuda_error(err, "factorization");
+    }
+  }
+  cudaFreeAsync(d_a, s);
+  if (d_b) cudaFreeAsync(d_b, s);
+  cudaFreeAsync(d_perm, s);
+  cudaFreeAsync(d_pt, s);
+  cudaFreeAsync(d_pe, s);
+  cudaFreeAsync(d_status, s);
+  cudaFreeAsync(ws, s);
+  cudaStreamSynchronize(s);
+  cudaStreamDestroy(s);
+  if (rc) return rc;
+  if (h_status != BBK_OK)
+    return set_error(h_status, "factorization aborted on the device: %s", bbk_status_string(h_status));
+  return BBK_OK;
+}
+
+int bbk_reconstruct_device(int n, const double* factors, long long ldf, const int* perm,
+                           const int* pivot_types, double* out, long long ldo, void* stream) {
+  if (n <= 0) return set_error(BBK_ERR_INVALID_ARGUMENT, "matrix size must be positive");
+  if (!factors || !perm || !pivot_types || !out || ldf < n || ldo < n)
+    return set_error(BBK_ERR_INVALID_ARGUMENT, "bad reconstruction arguments");
+  int rc = check_device();
+  if (rc) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  double* m = nullptr;
+  BBK_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&m),
+                               static_cast<size_t>(n) * n * sizeof(double), s));
+  rc = reconstruct_enqueue(n, factors, ldf, perm, pivot_types, out, ldo, m, s);
+  cudaFreeAsync(m, s);
+  if (rc) return rc;
+  BBK_CUDA_TRY(cudaStreamSynchronize(s));
+  return BBK_OK;
+}
+
+int bbk_scale_one_by_one(int count, double pivot, const double* source, int source_stride,
+                         double* destination, int destination_stride, void* stream) {
+  if (count <= 0) return BBK_OK;
+  if (!source || !destination) return set_error(BBK_ERR_INVALID_ARGUMENT, "null pointer");
+  int rc = check_device();
+  if (rc) return rc;
+  return launch_scale_1x1(count, pivot, source, source_stride, destination, destination_stride,
+                          static_cast<cudaStream_t>(stream));
+}
+
+int bbk_scale_two_by_two(int count, double a, double b, double c, const double* first_source,
+                         int first_source_stride, const double* second_source,
+                         int second_source_stride, double* first_destination,
+                         int first_destination_stride, double* second_destination,
+                         int second_destination_stride, void* stream) {
+  if (count <= 0) return BBK_OK;
+  if (!first_source || !second_source || !first_destination || !second_destination)
+    return set_error(BBK_ERR_INVALID_ARGUMENT, "null pointer");
+  int rc = check_device();
+  if (rc) return rc;
+  return launch_scale_2x2(count, a, b, c, first_source, first_source_stride, second_source,
+                          second_source_stride, first_destination, first_destination_stride,
+                          second_destination, second_destination_stride,
+                          static_cast<cudaStream_t>(stream));
+}
+
+int bbk_update_trailing_block(int rows, int cols, int inner_dim, const double* left_panel,
+                              int left_panel_stride, const double* workspace_panel,
+                              int workspace_panel_stride, double* target, int target_stride,
+                              int update_mode, void* stream) {
+  if (rows <= 0 || cols <= 0 || inner_dim <= 0) return BBK_OK;
+  if (!left_panel || !workspace_panel || !target)
+    return set_error(BBK_ERR_INVALID_ARGUMENT, "null pointer");
+  if (update_mode != BBK_UPDATE_FP64 && update_mode != BBK_UPDATE_FP64_ORDERED &&
+      update_mode != BBK_UPDATE_FP32)
+    return set_error(BBK_ERR_INVALID_ARGUMENT, "unknown update mode %d", update_mode);
+  int rc = check_device();
+  if (rc) return rc;
+  return launch_update_block(rows, cols, inner_dim, left_panel, left_panel_stride, workspace_panel,
+                             workspace_panel_stride, target, target_stride, update_mode,
+                             static_cast<cudaStream_t>(stream));
+}
+
+int bbk_probe_bounded_wait(int ctas, unsigned long long timeout_ns, void* stream) {
+  if (ctas <= 0 || ctas > kMaxPanelGrid || timeout_ns == 0)
+    return set_error(BBK_ERR_INVALID_ARGUMENT, "bad probe arguments");
+  int rc = check_device();
+  if (rc) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const size_t slot_words = 2ull * (ctas + 1) * kSlotWords;
+  const size_t bytes = align_up(sizeof(DeviceState), kAlign) + slot_words * 8;
+  char* base = nullptr;
+  BBK_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&base), bytes, s));
+  DeviceState* st = reinterpret_cast<DeviceState*>(base);
+  unsigned long long* slots =
+      reinterpret_cast<unsigned long long*>(base + align_up(sizeof(DeviceState), kAlign));
+  int h_status = BBK_OK;
+  cudaError_t err = cudaMemsetAsync(base, 0, bytes, s);
+  if (err != cudaSuccess) {
+    rc = cuda_error(err, "cudaMemsetAsync");
+  } else {
+    rc = launch_probe_wait(ctas, timeout_ns, st, slots, s);
+    if (!rc) {
+      err = cudaMemcpyAsync(&h_status, &st->status, sizeof(int), cudaMemcpyDeviceToHost, s);
+      if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+      if (err != cudaSuccess) rc = cuda_error(err, "probe");
+    }
+  }
+  cudaFreeAsync(base, s);
+  cudaStreamSynchronize(s);
+  if (rc) return rc;
+  if (h_status != BBK_OK) return set_error(h_status, "bounded wait expired as designed");
+  return set_error(BBK_ERR_LOGIC, "bounded-wait probe finished without timing out");
+}
+
+}  // extern "C"

@@ -1,0 +1,657 @@
+// Panel factorization of the blocked Bunch-Kaufman LDL^T: one persistent
+// cooperative launch per panel runs the panel's sequential pivot chain with
+// all CTAs, each owning a contiguous slice of the active columns [k0, n).
+//
+// Follows BlockLdltDecomposition::FactorPanel and its helpers
+// (src/block_ldlt_decomposition.cc:80-704 in wentianshu/BlockedBunchKaufmanLDLT)
+// in the reference's own operation order, so the panel's arithmetic is
+// bitwise identical to the reference (every product and sum separately
+// rounded; this file is also compiled with --fmad=false).
+//
+// Data during a panel whose first row is k0 (lp = p - k0 is the local pivot):
+//   A    n x lda row-major upper: rows >= p are the partially updated matrix;
+//        the panel's own rows stay frozen until finalize_kernel writes the
+//        compact factor rows into them.
+//   W    row lp holds the workspace row W[p, j] (j >= p) of pivot p.
+//   Ucm  column-major U: Ucm[j*ldu + lp] = U[p, j].  Column j belongs to the
+//        CTA that owns column j, so U[., r] is one contiguous read.
+//   Uout the final compact column of each pivot column of the panel
+//        (rows < lp from Ucm after the last interchange touching it, then D).
+//   wc   the candidate column W(i, r), i >= p.
+//
+// Per pivot step the grid meets once (no candidate) or twice (candidate
+// column needed).  Between one step's interchange/scaling phase and the next
+// step's row update there is no grid barrier: every write of the scaling phase
+// goes to a column its writer owns, except three kinds of value that the
+// next row update needs from other columns -- the next coefficients U[p, p']
+// (recomputed redundantly by every CTA from published scalars), the single
+// moved entry A[p', r] (read from the frozen row p instead), and a swapped
+// Ucm column (read from its pre-swap location).  Everything else is read
+// only after the next exchange.
+#include <climits>
+#include <cstdio>
+
+#include "bbk_internal.cuh"
+
+namespace bbk {
+namespace {
+
+constexpr int kThreads = 128;
+constexpr int kWarps = kThreads / 32;
+
+struct PanelArgs {
+  int n;
+  int panel;
+  int nominal_end;  // min((panel+1)*b, n)
+  int can_shift;    // another panel follows
+  double* a;
+  long long lda;
+  double* w;
+  long long ldw;
+  double* ucm;
+  int ldu;
+  double* uout;
+  double* wc;
+  int* perm;
+  int* ptype;
+  int* panel_end;
+  unsigned long long* slots;
+  DeviceState* st;
+  int nslots;        // records each exchange waits for (gridDim.x normally)
+  int slot_stride;   // records per parity in `slots` (>= nslots)
+  unsigned tag_base;
+  unsigned long long timeout_ns;
+};
+
+struct ExchangeOut {
+  double val;
+  int idx;
+  int ok;
+  double pub[kMaxPub];
+};
+
+__device__ __forceinline__ void fail(DeviceState* st, int code) {
+  atomicCAS(&st->status, 0, code);
+  atomicExch(&st->abort, 1);
+}
+
+// Spin until all `nw` words at p carry `tag`; false on abort or timeout.
+__device__ bool spin_tagged(const unsigned long long* p, int nw, unsigned tag,
+                            unsigned long long* out, DeviceState* st,
+                            unsigned long long t0, unsigned long long limit) {
+  for (unsigned iter = 1;; ++iter) {
+    bool ok = true;
+    for (int k = 0; k < nw; ++k) {
+      out[k] = ld_relaxed_u64(p + k);
+      ok &= static_cast<unsigned>(out[k] >> 32) == tag;
+    }
+    if (ok) return true;
+    if ((iter & 31u) == 0) {
+      if (ld_relaxed_s32(&st->abort)) return false;
+      if (globaltimer_ns() - t0 > limit) {
+        fail(st, BBK_ERR_TIMEOUT);
+        return false;
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ double join_hi_lo(unsigned long long hi, unsigned long long lo) {
+  const unsigned long long bits = ((hi & 0xffffffffull) << 32) | (lo & 0xffffffffull);
+  return __longlong_as_double(static_cast<long long>(bits));
+}
+
+// Argmax combine with the reference's tie rule (src/block_ldlt_decomposition.cc:
+// 164-182 scans ascending columns with a strict '>'): larger value wins, equal
+// values keep the lower index.  NaN never enters (callers skip it).
+__device__ __forceinline__ void argmax_join(double& v, int& i, double v2, int i2) {
+  if (v2 > v || (v2 == v && i2 < i)) {
+    v = v2;
+    i = i2;
+  }
+}
+
+// CTA-collective: reduce (my_val, my_idx) over the CTA, publish the CTA's
+// record (reduction + its kMaxPub scalars in pub_in), wait for the records of
+// all `nslots` CTAs, and return the grid-wide argmax plus pub[k] taken from
+// the record of CTA pub_owner[k].  Must be called by every thread.
+__device__ void exchange(const PanelArgs& P, unsigned tag, double my_val, int my_idx,
+                         const double* pub_in, const int* pub_owner, int npub,
+                         double* s_red_v, int* s_red_i, ExchangeOut* out) {
+  const int t = threadIdx.x;
+  const int lane = t & 31, warp = t >> 5;
+  for (int off = 16; off > 0; off >>= 1) {
+    const double v2 = __shfl_down_sync(0xffffffffu, my_val, off);
+    const int i2 = __shfl_down_sync(0xffffffffu, my_idx, off);
+    argmax_join(my_val, my_idx, v2, i2);
+  }
+  if (lane == 0) {
+    s_red_v[warp] = my_val;
+    s_red_i[warp] = my_idx;
+  }
+  __syncthreads();  // also orders this CTA's global writes before the fence
+  unsigned long long* rec =
+      P.slots + (static_cast<size_t>(tag & 1u) * P.slot_stride + blockIdx.x) * kSlotWords;
+  if (t == 0) {
+    double v = s_red_v[0];
+    int i = s_red_i[0];
+    for (int k = 1; k < kWarps; ++k) argmax_join(v, i, s_red_v[k], s_red_i[k]);
+    const unsigned long long bits = static_cast<unsigned long long>(__double_as_longlong(v));
+    fence_acq_rel_gpu();  // release everything this CTA wrote so far
+    st_relaxed_u64(rec + 0, tag_word(tag, static_cast<unsigned>(i)));
+    st_relaxed_u64(rec + 1, tag_word(tag, static_cast<unsigned>(bits >> 32)));
+    st_relaxed_u64(rec + 2, tag_word(tag, static_cast<unsigned>(bits)));
+    for (int k = 0; k < npub; ++k) {
+      const unsigned long long pb =
+          static_cast<unsigned long long>(__double_as_longlong(pub_in[k]));
+      st_relaxed_u64(rec + 3 + 2 * k, tag_word(tag, static_cast<unsigned>(pb >> 32)));
+      st_relaxed_u64(rec + 4 + 2 * k, tag_word(tag, static_cast<unsigned>(pb)));
+    }
+  }
+  if (warp == 0) {
+    const unsigned long long* base =
+        P.slots + static_cast<size_t>(tag & 1u) * P.slot_stride * kSlotWords;
+    const unsigned long long t0 = globaltimer_ns();
+    bool ok = true;
+    double v = 0.0;
+    int i = INT_MAX;
+    unsigned long long wbuf[3];
+    for (int s = lane; s < P.nslots && ok; s += 32) {
+      ok = spin_tagged(base + static_cast<size_t>(s) * kSlotWords, 3, tag, wbuf, P.st, t0,
+                       P.timeout_ns);
+      if (ok) argmax_join(v, i, join_hi_lo(wbuf[1], wbuf[2]), static_cast<int>(wbuf[0] & 0xffffffffu));
+    }
+    double pubv = 0.0;
+    if (ok && lane < npub) {
+      unsigned long long pw[2];
+      ok = spin_tagged(base + static_cast<size_t>(pub_owner[lane]) * kSlotWords + 3 + 2 * lane,
+                       2, tag, pw, P.st, t0, P.timeout_ns);
+      if (ok) pubv = join_hi_lo(pw[0], pw[1]);
+    }
+    fence_acq_rel_gpu();  // acquire what the other CTAs released
+    for (int off = 16; off > 0; off >>= 1) {
+      const double v2 = __shfl_down_sync(0xffffffffu, v, off);
+      const int i2 = __shfl_down_sync(0xffffffffu, i, off);
+      argmax_join(v, i, v2, i2);
+    }
+    const int all_ok = __all_sync(0xffffffffu, ok);
+    if (lane < npub) out->pub[lane] = pubv;
+    if (lane == 0) {
+      out->val = v;
+      out->idx = i;
+      out->ok = all_ok;
+    }
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ double safe_denominator(double d) {
+  // src/block_ldlt_decomposition.cc:21-26 (absolute threshold)
+  return fabs(d) <= kDblEpsilon ? 0.0 : d;
+}
+
+__device__ __forceinline__ double div_or_zero(double x, double den) {
+  return den == 0.0 ? 0.0 : xdiv(x, den);
+}
+
+__global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
+  __shared__ double s_red_v[kWarps];
+  __shared__ int s_red_i[kWarps];
+  __shared__ double s_pub[kMaxPub];
+  __shared__ ExchangeOut s_x;
+
+  if (ld_relaxed_s32(&P.st->abort)) return;
+  const int G = gridDim.x;
+  const int c = blockIdx.x;
+  const int t = threadIdx.x;
+  const int n = P.n;
+  const int kstart = ldcg(&P.st->kstart[P.panel & 1]);
+  const int S = (n - kstart + G - 1) / G;  // columns per CTA
+  const int lo = kstart + c * S;
+  const int hi = min(n, lo + S);
+  const long long lda = P.lda, ldw = P.ldw;
+  const int ldu = P.ldu;
+  auto owner = [&](int j) -> int { return (j - kstart) / S; };
+
+  unsigned tag = P.tag_base;
+  int p = kstart;
+  // coefficients U[q, p] of the current row: rows q < n_old from Ucm column
+  // coef_src, then n_extra (<= 2) values computed by every CTA.
+  int coef_src = p, n_old = 0, n_extra = 0;
+  double extra0 = 0.0, extra1 = 0.0;
+  int fix_col = -1;          // A[p][fix_col] must be read from fix_src
+  long long fix_src = 0;
+  int shifted = 0;
+
+  while (p < P.nominal_end) {
+    const int lp = p - kstart;
+    // ---- row update: W[p, j] = A[p, j] - sum_q U[q, p] W[q, j]
+    // (CopyCurrentRowToWorkspace + UpdateCurrentRowInWorkspace, :122-162)
+    double best = 0.0;
+    int best_j = INT_MAX;
+    if (t < kMaxPub) s_pub[t] = 0.0;
+    __syncthreads();
+    {
+      const double* ucol = P.ucm + static_cast<size_t>(coef_src) * ldu;
+      for (int j = max(lo, p) + t; j < hi; j += kThreads) {
+        double acc = 0.0;
+        for (int q = 0; q < n_old; ++q)
+          acc = xadd(acc, xmul(ldcg(ucol + q), ldcg(P.w + q * ldw + j)));
+        if (n_extra > 0) acc = xadd(acc, xmul(extra0, ldcg(P.w + n_old * ldw + j)));
+        if (n_extra > 1) acc = xadd(acc, xmul(extra1, ldcg(P.w + (n_old + 1) * ldw + j)));
+        const double av = (j == fix_col) ? ldcg(P.a + fix_src) : ldcg(P.a + p * lda + j);
+        const double wv = xsub(av, acc);
+        P.w[lp * ldw + j] = wv;
+        if (j > p) {
+          const double v = fabs(wv);
+          if (v > best) {  // FindCurrentRowMax, :164-182
+            best = v;
+            best_j = j;
+          }
+        } else {
+          s_pub[0] = wv;  // W[p, p]
+        }
+        if (j == p + 1) s_pub[1] = wv;
+        if (j == p + 2) s_pub[2] = wv;
+      }
+    }
+    fix_col = -1;
+    int owners[kMaxPub];
+    owners[0] = owner(p);
+    owners[1] = p + 1 < n ? owner(p + 1) : 0;
+    owners[2] = p + 2 < n ? owner(p + 2) : 0;
+    exchange(P, tag++, best, best_j, s_pub, owners, 3, s_red_v, s_red_i, &s_x);
+    if (!s_x.ok) return;
+    const double omega = s_x.val;
+    const int r = s_x.idx;
+    const double dpp = s_x.pub[0];
+    const double w_p1 = s_x.pub[1];  // W[p, p+1] (current-row version)
+    const double w_p2 = s_x.pub[2];  // W[p, p+2]
+    __syncthreads();
+
+    int kind = 1;  // 1: 1x1 at p; -1: 1x1 after p<->r; 2: 2x2 with p+1<->r
+    bool cand = false;
+    double wc_r = 0.0, wc_p = 0.0, wc_p1 = 0.0, wc_p2 = 0.0;
+    // FactorPanel's test, :90-92
+    if (!(fabs(dpp) >= xmul(kAlpha, omega) || omega == 0.0)) {
+      cand = true;
+      // ---- candidate column W(i, r) = A(i, r) - sum_q U[q, r] W[q, i]
+      // (CopyCandidateToWorkspace + UpdateCandidateInWorkspace, :184-352)
+      if (t < kMaxPub) s_pub[t] = 0.0;
+      __syncthreads();
+      double sig = 0.0;
+      const double* ucol = P.ucm + static_cast<size_t>(r) * ldu;
+      for (int i = max(lo, p) + t; i < hi; i += kThreads) {
+        double acc = 0.0;
+        for (int q = 0; q < lp; ++q)
+          acc = xadd(acc, xmul(ldcg(ucol + q), ldcg(P.w + q * ldw + i)));
+        const double av = i <= r ? ldcg(P.a + i * lda + r) : ldcg(P.a + r * lda + i);
+        const double v = xsub(av, acc);
+        P.wc[i] = v;
+        if (i != r) {
+          const double av2 = fabs(v);
+          sig = (sig < av2) ? av2 : sig;  // std::max, FindCandidateColumnMax :354-367
+        } else {
+          s_pub[0] = v;
+        }
+        if (i == p) s_pub[1] = v;
+        if (i == p + 1) s_pub[2] = v;
+        if (i == p + 2) s_pub[3] = v;
+      }
+      owners[0] = owner(r);
+      owners[1] = owner(p);
+      owners[2] = p + 1 < n ? owner(p + 1) : 0;
+      owners[3] = p + 2 < n ? owner(p + 2) : 0;
+      exchange(P, tag++, sig, 0, s_pub, owners, 4, s_red_v, s_red_i, &s_x);
+      if (!s_x.ok) return;
+      const double sigma = s_x.val;
+      wc_r = s_x.pub[0];
+      wc_p = s_x.pub[1];
+      wc_p1 = s_x.pub[2];
+      wc_p2 = s_x.pub[3];
+      __syncthreads();
+      // SelectPivot, :369-390
+      if (xsub(xmul(fabs(dpp), sigma), xmul(xmul(kAlpha, omega), omega)) >= 0.0) {
+        kind = 1;
+      } else if (xsub(fabs(wc_r), xmul(kAlpha, sigma)) >= 0.0) {
+        kind = -1;
+      } else {
+        kind = 2;
+      }
+      // :104-108: a 2x2 pivot starting at the panel's last column moves that
+      // column into the next panel (ShiftBoundaryColumnToNextBlock).
+      if (kind == 2 && p == P.nominal_end - 1 && P.can_shift) {
+        shifted = 1;
+        break;
+      }
+    }
+
+    if (kind == 1) {
+      // ScaleOneByOnePivot (:633-656); after a candidate evaluation the
+      // reference's W(p, r) holds the column version of that entry.
+      const double d = dpp;
+      const double den = safe_denominator(d);
+      for (int j = max(lo, p + 1) + t; j < hi; j += kThreads) {
+        double wv;
+        if (cand && j == r) {
+          wv = wc_p;
+          P.w[lp * ldw + j] = wv;
+        } else {
+          wv = P.w[lp * ldw + j];
+        }
+        P.ucm[static_cast<size_t>(j) * ldu + lp] = div_or_zero(wv, den);
+      }
+      if (c == owner(p)) {
+        for (int q = t; q < lp; q += kThreads)
+          P.uout[static_cast<size_t>(lp) * ldu + q] = ldcg(P.ucm + static_cast<size_t>(p) * ldu + q);
+        if (t == 0) {
+          P.uout[static_cast<size_t>(lp) * ldu + lp] = d;
+          P.ptype[p] = 1;
+        }
+      }
+      // next row's coefficients: U[q, p+1] for q < p, then U[p, p+1]
+      coef_src = p + 1;
+      n_old = lp;
+      n_extra = 1;
+      extra0 = div_or_zero((cand && r == p + 1) ? wc_p : w_p1, den);
+      p += 1;
+    } else if (kind == -1) {
+      // SwapOneByOnePivot (:392-401, :414-498) + ScaleOneByOnePivot.
+      const double d = wc_r;
+      const double den = safe_denominator(d);
+      for (int j = max(lo, p) + t; j < hi; j += kThreads) {
+        if (j == p) {
+          P.w[lp * ldw + j] = d;
+          continue;
+        }
+        const double wv = (j == r) ? wc_p : P.wc[j];
+        P.w[lp * ldw + j] = wv;
+        P.ucm[static_cast<size_t>(j) * ldu + lp] = div_or_zero(wv, den);
+        // old row p moves to row r (j > r) / column r (j < r); row p itself
+        // stays frozen so other CTAs may still read it.
+        const double old_apj = ldcg(P.a + p * lda + j);
+        if (j > r) {
+          P.a[r * lda + j] = old_apj;
+        } else if (j < r) {
+          P.a[j * lda + r] = old_apj;
+        } else {
+          P.a[r * lda + r] = ldcg(P.a + p * lda + p);
+        }
+      }
+      if (c == owner(r)) {
+        for (int q = t; q < lp; q += kThreads) {
+          const double ur = ldcg(P.ucm + static_cast<size_t>(r) * ldu + q);
+          P.uout[static_cast<size_t>(lp) * ldu + q] = ur;  // final column p
+          P.ucm[static_cast<size_t>(r) * ldu + q] = ldcg(P.ucm + static_cast<size_t>(p) * ldu + q);
+          P.w[q * ldw + r] = ldcg(P.w + q * ldw + p);
+        }
+      }
+      // previously factored rows: columns p and r exchange (:472-491)
+      for (int i = c * kThreads + t; i < kstart; i += G * kThreads) {
+        double* x = P.a + i * lda + p;
+        double* y = P.a + i * lda + r;
+        const double tx = *x;
+        *x = *y;
+        *y = tx;
+      }
+      if (c == 0 && t == 0) {
+        P.uout[static_cast<size_t>(lp) * ldu + lp] = d;
+        P.ptype[p] = 1;
+        const int tp = P.perm[p];
+        P.perm[p] = P.perm[r];
+        P.perm[r] = tp;
+      }
+      coef_src = (r == p + 1) ? p : p + 1;
+      n_old = lp;
+      n_extra = 1;
+      extra0 = div_or_zero((r == p + 1) ? wc_p : wc_p1, den);
+      if (p + 1 < r) {
+        fix_col = r;
+        fix_src = p * lda + (p + 1);  // new A[p+1, r] = old A[p, p+1]
+      }
+      p += 1;
+    } else {
+      // SwapTwoByTwoPivot (:403-412, :500-587) + ScaleTwoByTwoPivot (:658-704)
+      const int s = p + 1, ls = lp + 1;
+      const double d11 = dpp, d21 = wc_p, d22 = wc_r;
+      const double det = xsub(xmul(d11, d22), xmul(d21, d21));
+      const double i11 = xdiv(d22, det);
+      const double i22 = xdiv(d11, det);
+      const double i21 = xdiv(-d21, det);
+      for (int j = max(lo, p + 2) + t; j < hi; j += kThreads) {
+        double x;
+        if (j == r) {
+          x = w_p1;  // W(p, s) and W(p, r) exchange
+          P.w[lp * ldw + j] = x;
+        } else {
+          x = P.w[lp * ldw + j];
+        }
+        const double y = (j == r) ? wc_p1 : P.wc[j];
+        P.w[ls * ldw + j] = y;
+        P.ucm[static_cast<size_t>(j) * ldu + lp] = xadd(xmul(i11, x), xmul(i21, y));
+        P.ucm[static_cast<size_t>(j) * ldu + ls] = xadd(xmul(i21, x), xmul(i22, y));
+        if (r != s) {
+          const double old_asj = ldcg(P.a + s * lda + j);
+          if (j > r) {
+            P.a[r * lda + j] = old_asj;
+          } else if (j < r) {
+            P.a[j * lda + r] = old_asj;
+          } else {
+            P.a[r * lda + r] = ldcg(P.a + s * lda + s);
+          }
+        }
+      }
+      if (c == owner(p)) {
+        for (int q = t; q < lp; q += kThreads)
+          P.uout[static_cast<size_t>(lp) * ldu + q] = ldcg(P.ucm + static_cast<size_t>(p) * ldu + q);
+      }
+      if (c == owner(r)) {
+        for (int q = t; q < lp; q += kThreads) {
+          const double ur = ldcg(P.ucm + static_cast<size_t>(r) * ldu + q);
+          P.uout[static_cast<size_t>(ls) * ldu + q] = ur;  // final column s
+          if (r != s) {
+            P.ucm[static_cast<size_t>(r) * ldu + q] = ldcg(P.ucm + static_cast<size_t>(s) * ldu + q);
+            P.w[q * ldw + r] = ldcg(P.w + q * ldw + s);
+          }
+        }
+      }
+      if (r != s) {
+        for (int i = c * kThreads + t; i < kstart; i += G * kThreads) {
+          double* x = P.a + i * lda + s;
+          double* y = P.a + i * lda + r;
+          const double tx = *x;
+          *x = *y;
+          *y = tx;
+        }
+      }
+      if (c == 0 && t == 0) {
+        P.uout[static_cast<size_t>(lp) * ldu + lp] = d11;
+        P.uout[static_cast<size_t>(ls) * ldu + lp] = d21;
+        P.uout[static_cast<size_t>(ls) * ldu + ls] = d22;
+        P.ptype[p] = 2;
+        P.ptype[s] = -2;
+        const int tp = P.perm[s];
+        P.perm[s] = P.perm[r];
+        P.perm[r] = tp;
+      }
+      // next row p+2: coefficients U[q, p+2], q < p, then U[p, p+2], U[s, p+2]
+      const double x = (r == p + 2) ? w_p1 : w_p2;
+      const double y = (r == p + 2) ? wc_p1 : wc_p2;
+      coef_src = (r == p + 2) ? s : p + 2;
+      n_old = lp;
+      n_extra = 2;
+      extra0 = xadd(xmul(i11, x), xmul(i21, y));
+      extra1 = xadd(xmul(i21, x), xmul(i22, y));
+      if (p + 2 < r) {
+        fix_col = r;
+        fix_src = s * lda + (p + 2);  // new A[p+2, r] = old A[s, p+2]
+      }
+      p += 2;
+    }
+    __syncthreads();
+  }
+
+  if (c == 0 && t == 0) {
+    // panel range [kstart, p); the next panel starts at p.
+    P.st->kstart[(P.panel + 1) & 1] = p;
+    if (P.panel_end) P.panel_end[P.panel] = p;
+  }
+  (void)shifted;
+}
+
+// Writes the panel's compact factor rows [k0, e) into A:
+// A[q, j] = Uout (pivot columns j < e) or Ucm (trailing columns j >= e).
+constexpr int kFinTile = 32;
+__global__ void __launch_bounds__(256) finalize_kernel(double* a, long long lda, const double* ucm,
+                                                       int ldu, const double* uout, int n,
+                                                       DeviceState* st, int panel) {
+  __shared__ double tile[kFinTile][kFinTile + 1];
+  if (ld_relaxed_s32(&st->abort)) return;
+  const int k0 = ldcg(&st->kstart[panel & 1]);
+  const int e = ldcg(&st->kstart[(panel + 1) & 1]);
+  const int kb = e - k0;
+  if (kb <= 0) return;
+  // tiles over (q in [0, kb), j in [k0, n))
+  const int qt = (kb + kFinTile - 1) / kFinTile;
+  const int jt = (n - k0 + kFinTile - 1) / kFinTile;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+  for (int tileid = blockIdx.x; tileid < qt * jt; tileid += gridDim.x) {
+    const int q0 = (tileid % qt) * kFinTile;
+    const int j0 = k0 + (tileid / qt) * kFinTile;
+    // load: rows of the tile are columns j (contiguous in q)
+    for (int jj = ty; jj < kFinTile; jj += 8) {
+      const int j = j0 + jj, q = q0 + tx;
+      double v = 0.0;
+      if (j < n && q < kb) {
+        v = (j < e) ? uout[static_cast<size_t>(j - k0) * ldu + q]
+                    : ucm[static_cast<size_t>(j) * ldu + q];
+      }
+      tile[jj][tx] = v;
+    }
+    __syncthreads();
+    for (int qq = ty; qq < kFinTile; qq += 8) {
+      const int q = q0 + qq, j = j0 + tx;
+      if (q < kb && j < n && j >= k0 + q) a[static_cast<size_t>(k0 + q) * lda + j] = tile[tx][qq];
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void init_kernel(int n, int* perm, int* pivot_types, DeviceState* st,
+                            unsigned long long* slots, size_t slot_words) {
+  const size_t i0 = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
+  for (size_t i = i0; i < static_cast<size_t>(n); i += stride) {
+    perm[i] = static_cast<int>(i);
+    pivot_types[i] = 0;
+  }
+  for (size_t i = i0; i < slot_words; i += stride) slots[i] = 0ull;
+  if (i0 == 0) {
+    st->kstart[0] = 0;
+    st->kstart[1] = 0;
+    st->abort = 0;
+    st->status = 0;
+  }
+}
+
+__global__ void status_copy_kernel(const DeviceState* st, int* out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *out = st->status;
+}
+
+// Bounded-wait probe: one exchange that also waits for a record nobody
+// writes (nslots = gridDim.x + 1), so it must end by timeout.
+__global__ void __launch_bounds__(kThreads) probe_kernel(PanelArgs P) {
+  __shared__ double s_red_v[kWarps];
+  __shared__ int s_red_i[kWarps];
+  __shared__ double s_pub[kMaxPub];
+  __shared__ ExchangeOut s_x;
+  if (threadIdx.x < kMaxPub) s_pub[threadIdx.x] = 0.0;
+  int owners[kMaxPub] = {0, 0, 0, 0, 0, 0};
+  __syncthreads();
+  exchange(P, P.tag_base, 0.0, 0, s_pub, owners, 0, s_red_v, s_red_i, &s_x);
+}
+
+}  // namespace
+
+static int cooperative_launch(const void* fn, int grid, PanelArgs* args, cudaStream_t s) {
+  void* kargs[] = {args};
+  cudaError_t err = cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kThreads), kargs, 0, s);
+  if (err != cudaSuccess) return cuda_error(err, "cudaLaunchCooperativeKernel(panel)");
+  count_launch();
+  return BBK_OK;
+}
+
+int panel_grid_size(int n) {
+  // enough CTAs that each owns <= 128 columns, at most one per SM
+  const int sms = device_sm_count();
+  int g = (n + 63) / 64;
+  if (g > sms) g = sms;
+  if (g < 1) g = 1;
+  return g;
+}
+
+int launch_init(int n, int* perm, int* pivot_types, DeviceState* st, unsigned long long* slots,
+                size_t slot_words, cudaStream_t s) {
+  init_kernel<<<256, 256, 0, s>>>(n, perm, pivot_types, st, slots, slot_words);
+  BBK_CUDA_TRY(cudaGetLastError());
+  count_launch();
+  return BBK_OK;
+}
+
+int launch_panel(const FactorPlan& plan, int panel, cudaStream_t s) {
+  PanelArgs P{};
+  P.n = plan.n;
+  P.panel = panel;
+  const long long nominal = static_cast<long long>(panel + 1) * plan.b;
+  P.nominal_end = nominal < plan.n ? static_cast<int>(nominal) : plan.n;
+  P.can_shift = panel + 1 < plan.nb;
+  P.a = plan.a;
+  P.lda = plan.lda;
+  P.w = plan.w;
+  P.ldw = plan.ldw;
+  P.ucm = plan.ucm;
+  P.ldu = plan.ldu;
+  P.uout = plan.uout;
+  P.wc = plan.wc;
+  P.perm = plan.perm;
+  P.ptype = plan.pivot_types;
+  P.panel_end = plan.panel_end;
+  P.slots = plan.slots;
+  P.st = plan.state;
+  P.nslots = plan.grid;
+  P.slot_stride = plan.grid;
+  // tags: distinct for every exchange of the call (slots are zeroed per call)
+  P.tag_base = 1u + static_cast<unsigned>(panel) * (2u * static_cast<unsigned>(plan.b) + 8u);
+  P.timeout_ns = plan.timeout_ns;
+  return cooperative_launch(reinterpret_cast<const void*>(panel_kernel), plan.grid, &P, s);
+}
+
+int launch_finalize(const FactorPlan& plan, int panel, cudaStream_t s) {
+  const int sms = device_sm_count();
+  finalize_kernel<<<2 * sms, 256, 0, s>>>(plan.a, plan.lda, plan.ucm, plan.ldu, plan.uout,
+                                          plan.n, plan.state, panel);
+  BBK_CUDA_TRY(cudaGetLastError());
+  count_launch();
+  return BBK_OK;
+}
+
+int launch_status_copy(const DeviceState* st, int* status_out, cudaStream_t s) {
+  status_copy_kernel<<<1, 32, 0, s>>>(st, status_out);
+  BBK_CUDA_TRY(cudaGetLastError());
+  count_launch();
+  return BBK_OK;
+}
+
+int launch_probe_wait(int ctas, unsigned long long timeout_ns, DeviceState* st,
+                      unsigned long long* slots, cudaStream_t s) {
+  PanelArgs P{};
+  P.slots = slots;
+  P.st = st;
+  P.nslots = ctas + 1;  // one participant that never arrives
+  P.slot_stride = ctas + 1;
+  P.tag_base = 7u;
+  P.timeout_ns = timeout_ns;
+  return cooperative_launch(reinterpret_cast<const void*>(probe_kernel), ctas, &P, s);
+}
+
+}  // namespace bbk

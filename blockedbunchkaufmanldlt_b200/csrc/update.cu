@@ -1,0 +1,495 @@
+// Trailing update A22 -= U^T W of the blocked Bunch-Kaufman LDL^T
+// (UpdateTrailingBlocks + kernels::UpdateTrailingBlock,
+// src/block_ldlt_decomposition.cc:706-744 and src/kernels.cc:67-91 in
+// wentianshu/BlockedBunchKaufmanLDLT), plus the standalone kernels.h entry
+// points (ScaleOneByOnePivot / ScaleTwoByTwoPivot / UpdateTrailingBlock).
+//
+// C(i,j) -= sum_k A(i,k) B(k,j) with A(i,k) = U[k, i] and B(k,j) = W[k, j].
+// Three arithmetics:
+//   FP64          FP64 tensor cores: mma.sync.m16n8k8.f64 from shared-memory
+//                 tiles staged with cp.async (double-buffered); 64x64 C tile
+//                 per CTA, 32x32 per warp.
+//   FP64_ORDERED  SIMT, every product and sum rounded separately with k
+//                 ascending and one final subtraction: bitwise the
+//                 reference's arithmetic.
+//   FP32          operands rounded to FP32, FP32 FMA accumulation, the result
+//                 subtracted in FP64.
+// In the factorization the C tiles cover the upper triangle of the trailing
+// matrix only (the reference also fills the unused lower halves of its
+// diagonal blocks; nothing ever reads them).
+#include <algorithm>
+
+#include "bbk_internal.cuh"
+
+namespace bbk {
+namespace {
+
+constexpr int kBM = 64, kBN = 64, kBK = 32;
+constexpr int kThreadsMma = 128;
+constexpr int kPadA = 4, kPadB = 4;  // leading dims = 4 (mod 16) doubles: conflict-free fragments
+
+struct UpdArgs {
+  // A(i,k) = a[i*a_si + k*a_sk], B(k,j) = b[k*b_sk + j], C(i,j) = c[i*ldc + j]
+  const double* a;
+  long long a_si, a_sk;
+  const double* b;
+  long long b_sk;
+  double* c;
+  long long ldc;
+  int i_lo, i_hi, j_lo, j_hi, inner;
+  int upper_only;  // only write i <= j
+  int tile_i0, tile_j0;  // origin of the tile grid (tile rows/cols start here)
+  int tiles_m, tiles_n;  // tile grid extent (rectangular mode)
+  int triangular;        // enumerate tiles (I <= J) of a square grid of tiles_m
+  // panel mode: read the range from the device state
+  const DeviceState* st;
+  int panel;
+  int n;
+};
+
+__device__ __forceinline__ void cp_async_8(double* smem_dst, const double* gsrc, bool valid) {
+  const unsigned saddr = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  const int src_bytes = valid ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(saddr), "l"(gsrc),
+               "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_16(double* smem_dst, const double* gsrc, int src_bytes) {
+  const unsigned saddr = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(saddr), "l"(gsrc),
+               "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Resolve the panel-mode range from the device state.
+__device__ __forceinline__ bool resolve_range(UpdArgs& U) {
+  if (U.st == nullptr) return true;
+  if (ld_relaxed_s32(&U.st->abort)) return false;
+  const int k0 = ldcg(&U.st->kstart[U.panel & 1]);
+  const int e = ldcg(&U.st->kstart[(U.panel + 1) & 1]);
+  U.inner = e - k0;
+  U.i_lo = U.j_lo = e;
+  U.i_hi = U.j_hi = U.n;
+  U.tile_i0 = U.tile_j0 = (e / kBM) * kBM;
+  U.tiles_m = U.tiles_n = (U.n - U.tile_i0 + kBM - 1) / kBM;
+  // Ucm/W hold rows q relative to the panel start.
+  return U.inner > 0 && e < U.n;
+}
+
+__device__ __forceinline__ int tile_count(const UpdArgs& U) {
+  return U.triangular ? U.tiles_m * (U.tiles_m + 1) / 2 : U.tiles_m * U.tiles_n;
+}
+
+__device__ __forceinline__ void tile_coords(const UpdArgs& U, int t, int& I, int& J) {
+  if (!U.triangular) {
+    I = t % U.tiles_m;
+    J = t / U.tiles_m;
+    return;
+  }
+  // column-major over the upper triangle: J(J+1)/2 <= t < (J+1)(J+2)/2
+  int j = static_cast<int>((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+  while (j * (j + 1) / 2 > t) --j;
+  while ((j + 1) * (j + 2) / 2 <= t) ++j;
+  J = j;
+  I = t - j * (j + 1) / 2;
+}
+
+// ---------------------------------------------------------------------------
+// FP64 tensor-core tile
+// ---------------------------------------------------------------------------
+template <bool kAK>  // true: A contiguous along k (a_sk == 1); false: along i
+struct MmaSmem {
+  static constexpr int kAStride = kAK ? (kBK + kPadA) : (kBM + kPadA);
+  static constexpr int kASize = kAK ? kBM * kAStride : kBK * kAStride;
+  static constexpr int kBStride = kBN + kPadB;
+  static constexpr int kBSize = kBK * kBStride;
+  static constexpr int kStage = kASize + kBSize;
+  static constexpr size_t kBytes = 2 * kStage * sizeof(double);
+  __device__ static double& a_at(double* as, int i, int k) {
+    return kAK ? as[i * kAStride + k] : as[k * kAStride + i];
+  }
+};
+
+template <bool kAK, bool kVec>
+__device__ __forceinline__ void load_stage(const UpdArgs& U, double* as, double* bs, int i0, int j0,
+                                           int k0) {
+  using Sm = MmaSmem<kAK>;
+  const int t = threadIdx.x;
+  if (kVec) {
+    // A: 64 rows x 32 k, contiguous along k, 16-byte chunks (2 doubles)
+    for (int c = t; c < kBM * (kBK / 2); c += kThreadsMma) {
+      const int ii = c / (kBK / 2), kk = (c % (kBK / 2)) * 2;
+      const int k = k0 + kk;
+      const int nvalid = max(0, min(2, U.inner - k));
+      const double* src = U.a + static_cast<long long>(i0 + ii) * U.a_si + (nvalid ? k : 0);
+      cp_async_16(&as[ii * Sm::kAStride + kk], src, nvalid * 8);
+    }
+    // B: 32 k x 64 j
+    for (int c = t; c < kBK * (kBN / 2); c += kThreadsMma) {
+      const int kk = c / (kBN / 2), jj = (c % (kBN / 2)) * 2;
+      const int k = k0 + kk;
+      const bool ok = k < U.inner;
+      const double* src = U.b + static_cast<long long>(ok ? k : 0) * U.b_sk + j0 + jj;
+      cp_async_16(&bs[kk * Sm::kBStride + jj], src, ok ? 16 : 0);
+    }
+  } else {
+    for (int c = t; c < kBM * kBK; c += kThreadsMma) {
+      int ii, kk;
+      if (kAK) {
+        ii = c / kBK;
+        kk = c % kBK;
+      } else {
+        kk = c / kBM;
+        ii = c % kBM;
+      }
+      const int i = i0 + ii, k = k0 + kk;
+      const bool ok = k < U.inner && i >= U.i_lo && i < U.i_hi;
+      const double* src = ok ? U.a + static_cast<long long>(i) * U.a_si + static_cast<long long>(k) * U.a_sk : U.a;
+      cp_async_8(&Sm::a_at(as, ii, kk), src, ok);
+    }
+    for (int c = t; c < kBK * kBN; c += kThreadsMma) {
+      const int kk = c / kBN, jj = c % kBN;
+      const int j = j0 + jj, k = k0 + kk;
+      const bool ok = k < U.inner && j >= U.j_lo && j < U.j_hi;
+      const double* src = ok ? U.b + static_cast<long long>(k) * U.b_sk + j : U.b;
+      cp_async_8(&bs[kk * Sm::kBStride + jj], src, ok);
+    }
+  }
+  cp_async_commit();
+}
+
+__device__ __forceinline__ void mma_16x8x8(double (&c)[4], const double (&a)[4], const double (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};"
+      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+}
+
+template <bool kAK, bool kVec>
+__device__ void mma_tile(const UpdArgs& U, double* smem, int I, int J) {
+  using Sm = MmaSmem<kAK>;
+  const int i0 = U.tile_i0 + I * kBM, j0 = U.tile_j0 + J * kBN;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, tq = lane & 3;
+  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+  double acc[2][4][4];
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.0;
+
+  const int nchunks = (U.inner + kBK - 1) / kBK;
+  double* st0 = smem;
+  double* st1 = smem + Sm::kStage;
+  load_stage<kAK, kVec>(U, st0, st0 + Sm::kASize, i0, j0, 0);
+  for (int ch = 0; ch < nchunks; ++ch) {
+    double* cur = (ch & 1) ? st1 : st0;
+    if (ch + 1 < nchunks) {
+      double* nxt = (ch & 1) ? st0 : st1;
+      load_stage<kAK, kVec>(U, nxt, nxt + Sm::kASize, i0, j0, (ch + 1) * kBK);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    double* as = cur;
+    double* bs = cur + Sm::kASize;
+#pragma unroll
+    for (int ks = 0; ks < kBK; ks += 8) {
+      double af[2][4], bf[4][2];
+#pragma unroll
+      for (int mt = 0; mt < 2; ++mt) {
+        const int r = wm + mt * 16 + g;
+        af[mt][0] = Sm::a_at(as, r, ks + tq);
+        af[mt][1] = Sm::a_at(as, r + 8, ks + tq);
+        af[mt][2] = Sm::a_at(as, r, ks + tq + 4);
+        af[mt][3] = Sm::a_at(as, r + 8, ks + tq + 4);
+      }
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) {
+        const int col = wn + nt * 8 + g;
+        bf[nt][0] = bs[(ks + tq) * Sm::kBStride + col];
+        bf[nt][1] = bs[(ks + tq + 4) * Sm::kBStride + col];
+      }
+#pragma unroll
+      for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) mma_16x8x8(acc[mt][nt], af[mt], bf[nt]);
+    }
+    __syncthreads();
+  }
+  // C -= acc on the valid part of the tile
+#pragma unroll
+  for (int mt = 0; mt < 2; ++mt) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int i = i0 + wm + mt * 16 + g + h * 8;
+      if (i < U.i_lo || i >= U.i_hi) continue;
+      double* crow = U.c + static_cast<long long>(i) * U.ldc;
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) {
+        const int j = j0 + wn + nt * 8 + tq * 2;
+        const double v0 = acc[mt][nt][h * 2], v1 = acc[mt][nt][h * 2 + 1];
+        const bool ok0 = j >= U.j_lo && j < U.j_hi && (!U.upper_only || i <= j);
+        const bool ok1 = j + 1 >= U.j_lo && j + 1 < U.j_hi && (!U.upper_only || i <= j + 1);
+        if (kVec && ok0 && ok1) {
+          double2* p2 = reinterpret_cast<double2*>(crow + j);
+          double2 cv = *p2;
+          cv.x -= v0;
+          cv.y -= v1;
+          *p2 = cv;
+        } else {
+          if (ok0) crow[j] -= v0;
+          if (ok1) crow[j + 1] -= v1;
+        }
+      }
+    }
+  }
+}
+
+template <bool kAK, bool kVec>
+__global__ void __launch_bounds__(kThreadsMma) mma_update_kernel(UpdArgs U) {
+  extern __shared__ double smem[];
+  if (!resolve_range(U)) return;
+  const int ntiles = tile_count(U);
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    int I, J;
+    tile_coords(U, t, I, J);
+    mma_tile<kAK, kVec>(U, smem, I, J);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// SIMT tiles: reference-ordered FP64 and FP32.  256 threads, 4x4 per thread.
+// ---------------------------------------------------------------------------
+constexpr int kThreadsSimt = 256;
+constexpr int kSK = 16;  // k chunk
+
+template <typename T, bool kOrdered>
+__device__ void simt_tile(const UpdArgs& U, T* as, T* bs, int I, int J) {
+  // as[kSK][kBM], bs[kSK][kBN]
+  const int i0 = U.tile_i0 + I * kBM, j0 = U.tile_j0 + J * kBN;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  T acc[4][4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) acc[r][c] = T(0);
+  for (int k0 = 0; k0 < U.inner; k0 += kSK) {
+    for (int c = threadIdx.x; c < kSK * kBM; c += kThreadsSimt) {
+      const int kk = c / kBM, ii = c % kBM;
+      const int i = i0 + ii, k = k0 + kk;
+      const bool ok = k < U.inner && i >= U.i_lo && i < U.i_hi;
+      as[kk * kBM + ii] =
+          ok ? T(U.a[static_cast<long long>(i) * U.a_si + static_cast<long long>(k) * U.a_sk]) : T(0);
+    }
+    for (int c = threadIdx.x; c < kSK * kBN; c += kThreadsSimt) {
+      const int kk = c / kBN, jj = c % kBN;
+      const int j = j0 + jj, k = k0 + kk;
+      const bool ok = k < U.inner && j >= U.j_lo && j < U.j_hi;
+      bs[kk * kBN + jj] = ok ? T(U.b[static_cast<long long>(k) * U.b_sk + j]) : T(0);
+    }
+    __syncthreads();
+    const int kmax = min(kSK, U.inner - k0);
+    for (int kk = 0; kk < kmax; ++kk) {
+      T av[4], bv[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) av[r] = as[kk * kBM + ty + 16 * r];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) bv[c] = bs[kk * kBN + tx + 16 * c];
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          if (kOrdered) {
+            acc[r][c] = xadd(acc[r][c], xmul(av[r], bv[c]));
+          } else {
+            acc[r][c] = fmaf(av[r], bv[c], acc[r][c]);
+          }
+        }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const int i = i0 + ty + 16 * r;
+    if (i < U.i_lo || i >= U.i_hi) continue;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int j = j0 + tx + 16 * c;
+      if (j < U.j_lo || j >= U.j_hi || (U.upper_only && i > j)) continue;
+      double* p = U.c + static_cast<long long>(i) * U.ldc + j;
+      if (kOrdered) {
+        *p = xsub(*p, acc[r][c]);
+      } else {
+        *p = *p - static_cast<double>(acc[r][c]);
+      }
+    }
+  }
+}
+
+template <typename T, bool kOrdered>
+__global__ void __launch_bounds__(kThreadsSimt) simt_update_kernel(UpdArgs U) {
+  __shared__ T as[kSK * kBM];
+  __shared__ T bs[kSK * kBN];
+  if (!resolve_range(U)) return;
+  const int ntiles = tile_count(U);
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    int I, J;
+    tile_coords(U, t, I, J);
+    simt_tile<T, kOrdered>(U, as, bs, I, J);
+  }
+}
+
+template <bool kAK, bool kVec>
+int launch_mma(const UpdArgs& U, int grid, cudaStream_t s) {
+  static bool configured = false;
+  const size_t bytes = MmaSmem<kAK>::kBytes;
+  if (!configured) {
+    BBK_CUDA_TRY(cudaFuncSetAttribute(mma_update_kernel<kAK, kVec>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(bytes)));
+    configured = true;
+  }
+  mma_update_kernel<kAK, kVec><<<grid, kThreadsMma, bytes, s>>>(U);
+  BBK_CUDA_TRY(cudaGetLastError());
+  count_launch();
+  return BBK_OK;
+}
+
+int launch_by_mode(const UpdArgs& U, int mode, bool ak, bool vec, int grid_mma, int grid_simt,
+                   cudaStream_t s) {
+  switch (mode) {
+    case BBK_UPDATE_FP64:
+      if (ak && vec) return launch_mma<true, true>(U, grid_mma, s);
+      if (ak) return launch_mma<true, false>(U, grid_mma, s);
+      return launch_mma<false, false>(U, grid_mma, s);
+    case BBK_UPDATE_FP64_ORDERED:
+      simt_update_kernel<double, true><<<grid_simt, kThreadsSimt, 0, s>>>(U);
+      break;
+    case BBK_UPDATE_FP32:
+      simt_update_kernel<float, false><<<grid_simt, kThreadsSimt, 0, s>>>(U);
+      break;
+    default:
+      return set_error(BBK_ERR_INVALID_ARGUMENT, "unknown update mode %d", mode);
+  }
+  BBK_CUDA_TRY(cudaGetLastError());
+  count_launch();
+  return BBK_OK;
+}
+
+// ---------------------------------------------------------------------------
+// kernels::ScaleOneByOnePivot / ScaleTwoByTwoPivot (src/kernels.cc:11-65)
+// ---------------------------------------------------------------------------
+__global__ void scale_1x1_kernel(int count, double pivot, const double* src, int ss, double* dst,
+                                 int ds) {
+  const bool zero = fabs(pivot) == 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    dst[static_cast<long long>(i) * ds] =
+        zero ? 0.0 : xdiv(src[static_cast<long long>(i) * ss], pivot);
+  }
+}
+
+__global__ void scale_2x2_kernel(int count, double a, double b, double c, const double* s1,
+                                 int s1s, const double* s2, int s2s, double* d1, int d1s,
+                                 double* d2, int d2s) {
+  const double det = xsub(xmul(a, c), xmul(b, b));
+  const bool zero = fabs(det) == 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    const double x = s1[static_cast<long long>(i) * s1s];
+    const double y = s2[static_cast<long long>(i) * s2s];
+    // (x*c - y*b)/det and (-x*b + y*a)/det, as src/kernels.cc:57-63
+    d1[static_cast<long long>(i) * d1s] = zero ? 0.0 : xdiv(xsub(xmul(x, c), xmul(y, b)), det);
+    d2[static_cast<long long>(i) * d2s] = zero ? 0.0 : xdiv(xadd(xmul(-x, b), xmul(y, a)), det);
+  }
+}
+
+}  // namespace
+
+int launch_update(const FactorPlan& plan, int panel, cudaStream_t s) {
+  if (panel + 1 >= plan.nb) return BBK_OK;  // nothing trails the last panel
+  UpdArgs U{};
+  U.a = plan.ucm;
+  U.a_si = plan.ldu;
+  U.a_sk = 1;
+  U.b = plan.w;
+  U.b_sk = plan.ldw;
+  U.c = plan.a;
+  U.ldc = plan.lda;
+  U.upper_only = 1;
+  U.triangular = 1;
+  U.st = plan.state;
+  U.panel = panel;
+  U.n = plan.n;
+  const int sms = device_sm_count();
+  // tiles of the first trailing panel bound the work; persistent grid
+  const long long nominal_e = std::max(0LL, static_cast<long long>(panel + 1) * plan.b - 1);
+  const long long tm = (plan.n - (nominal_e / kBM) * kBM + kBM - 1) / kBM;
+  const long long tiles = tm * (tm + 1) / 2;
+  const int grid_mma = static_cast<int>(std::max(1LL, std::min<long long>(tiles, 3LL * sms)));
+  const int grid_simt = static_cast<int>(std::max(1LL, std::min<long long>(tiles, 4LL * sms)));
+  // vector path needs 16-byte aligned rows: ldu, ldw, lda even and a/c 16-byte aligned
+  const bool vec = (plan.ldu % 2 == 0) && (plan.ldw % 2 == 0) && (plan.lda % 2 == 0) &&
+                   (reinterpret_cast<uintptr_t>(plan.a) % 16 == 0);
+  return launch_by_mode(U, plan.mode, true, vec, grid_mma, grid_simt, s);
+}
+
+int launch_update_block(int rows, int cols, int inner, const double* left, int ls,
+                        const double* ws, int wss, double* target, int ts, int mode,
+                        cudaStream_t s) {
+  if (rows <= 0 || cols <= 0 || inner <= 0) return BBK_OK;
+  UpdArgs U{};
+  U.a = left;
+  U.a_si = 1;
+  U.a_sk = ls;
+  U.b = ws;
+  U.b_sk = wss;
+  U.c = target;
+  U.ldc = ts;
+  U.i_lo = 0;
+  U.i_hi = rows;
+  U.j_lo = 0;
+  U.j_hi = cols;
+  U.inner = inner;
+  U.upper_only = 0;
+  U.triangular = 0;
+  U.tile_i0 = 0;
+  U.tile_j0 = 0;
+  U.tiles_m = (rows + kBM - 1) / kBM;
+  U.tiles_n = (cols + kBN - 1) / kBN;
+  const int sms = device_sm_count();
+  const long long tiles = static_cast<long long>(U.tiles_m) * U.tiles_n;
+  const int grid = static_cast<int>(std::max(1LL, std::min<long long>(tiles, 4LL * sms)));
+  return launch_by_mode(U, mode, false, false, grid, grid, s);
+}
+
+int launch_scale_1x1(int count, double pivot, const double* src, int ss, double* dst, int ds,
+                     cudaStream_t s) {
+  if (count <= 0) return BBK_OK;
+  const int grid = std::min(1024, (count + 255) / 256);
+  scale_1x1_kernel<<<grid, 256, 0, s>>>(count, pivot, src, ss, dst, ds);
+  BBK_CUDA_TRY(cudaGetLastError());
+  count_launch();
+  return BBK_OK;
+}
+
+int launch_scale_2x2(int count, double a, double b, double c, const double* s1, int s1s,
+                     const double* s2, int s2s, double* d1, int d1s, double* d2, int d2s,
+                     cudaStream_t s) {
+  if (count <= 0) return BBK_OK;
+  const int grid = std::min(1024, (count + 255) / 256);
+  scale_2x2_kernel<<<grid, 256, 0, s>>>(count, a, b, c, s1, s1s, s2, s2s, d1, d1s, d2, d2s);
+  BBK_CUDA_TRY(cudaGetLastError());
+  count_launch();
+  return BBK_OK;
+}
+
+}  // namespace bbk

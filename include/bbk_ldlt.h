@@ -1,0 +1,169 @@
+/*
+ * bbk_ldlt.h -- C ABI of the B200-native blocked Bunch-Kaufman LDL^T library
+ * (libbbk_b200.so).  Plain pointers, sizes and status codes only; every entry
+ * point is `extern "C"` and safe to bind from ctypes, cgo, JNI or C.
+ *
+ * Storage convention shared by every entry point: a symmetric matrix of
+ * order n is an n x lda row-major array whose upper triangle (i <= j) holds
+ * the matrix, which is the dense equivalent of the reference's BlockMatrix
+ * upper-block storage (include/block_matrix.h:24-72 in
+ * wentianshu/BlockedBunchKaufmanLDLT).  The strict lower triangle is never
+ * read; the factorization uses it as scratch only where stated.
+ *
+ * Compact factors: after factorization the upper triangle holds D on the
+ * diagonal and, for a 2x2 pivot starting at k, D(k,k+1) at (k,k+1); every
+ * other strictly-upper entry (k,i) holds U(k,i) = L(i,k).  perm[i] is the
+ * original index at factored position i, so (P A P^T)(i,j) = A(perm[i],
+ * perm[j]) = (L D L^T)(i,j); pivot_types[i] is 1, 2 (first of a 2x2) or -2
+ * (second of a 2x2).  This is exactly the reference's compact layout
+ * (src/block_ldlt_decomposition.cc:633-704, tests/block_ldlt_decomposition_
+ * test.cc:421-450).
+ *
+ * Errors: every function returns a bbk_status; bbk_last_error() gives a
+ * thread-local message.  The C++ surface (include/block_ldlt_decomposition.h)
+ * maps these onto the reference's exception types.
+ */
+#ifndef BBK_LDLT_H_
+#define BBK_LDLT_H_
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BBK_ABI_VERSION 1
+
+typedef enum bbk_status {
+  BBK_OK = 0,
+  BBK_ERR_INVALID_ARGUMENT = 1, /* reference: std::invalid_argument */
+  BBK_ERR_OUT_OF_RANGE = 2,     /* reference: std::out_of_range */
+  BBK_ERR_LOGIC = 3,            /* reference: std::logic_error */
+  BBK_ERR_ALLOC = 4,            /* reference: std::bad_alloc */
+  BBK_ERR_CUDA = 5,             /* a CUDA runtime call failed */
+  BBK_ERR_TIMEOUT = 6,          /* a device-side bounded wait ran out */
+  BBK_ERR_NO_DEVICE = 7,        /* no usable sm_100 device */
+  BBK_ERR_WORKSPACE = 8         /* caller workspace smaller than required */
+} bbk_status;
+
+/* Arithmetic of the trailing update A22 -= U^T W.  The panel (pivot search,
+ * interchanges, scaling, in-panel row updates) is always FP64 in the
+ * reference's own operation order. */
+typedef enum bbk_update_mode {
+  BBK_UPDATE_FP64 = 0,         /* FP64 tensor cores (DMMA mma.sync f64) */
+  BBK_UPDATE_FP64_ORDERED = 1, /* FP64, reference summation order: bitwise
+                                  identical to the reference */
+  BBK_UPDATE_FP32 = 2          /* operands rounded to FP32, FP32 accumulate,
+                                  result subtracted in FP64 */
+} bbk_update_mode;
+
+/* ---- version / diagnostics ------------------------------------------- */
+int bbk_abi_version(void);
+const char* bbk_last_error(void);
+const char* bbk_status_string(int status);
+/* Number of kernels this library has launched in this process. */
+unsigned long long bbk_kernel_launch_count(void);
+/* Upper bound, in nanoseconds, on every device-side spin wait (grid-wide
+ * pivot exchanges).  A wait that runs out aborts the factorization with
+ * BBK_ERR_TIMEOUT instead of hanging.  Default 5 s. */
+int bbk_set_wait_timeout_ns(unsigned long long timeout_ns);
+/* Test hook for the bounded-wait machinery: launches one cooperative grid of
+ * `ctas` blocks whose exchange also waits for one participant that does not
+ * exist, so the wait must run out.  Returns BBK_ERR_TIMEOUT when the bound
+ * works (and leaves the context usable), BBK_OK never. */
+int bbk_probe_bounded_wait(int ctas, unsigned long long timeout_ns, void* stream);
+
+/* ---- factorization ------------------------------------------------------
+ * Replaces BlockLdltDecomposition(const BlockMatrix&, mode) + Factorize()
+ * (reference include/block_ldlt_decomposition.h:18-23,
+ * src/block_ldlt_decomposition.cc:30-59).  `block_size` is the reference's
+ * BlockMatrix block size: it sets the panel width, the panel boundaries
+ * (and so the same pivot sequence and boundary shifts as the reference).
+ *
+ * Device variant: a, perm, pivot_types, panel_end are device pointers;
+ * panel_end (ceil(n/block_size) ints, may be NULL) receives the first row
+ * after each panel, from which the reference's block geometry (boundary
+ * shifts, src/block_ldlt_decomposition.cc:589-631) follows.  `workspace`
+ * may be NULL (the library allocates with cudaMallocAsync on `stream`),
+ * else it must hold bbk_factor_workspace_size(n, block_size) bytes.  The call
+ * enqueues on `stream` and then waits for it, returning the device status. */
+size_t bbk_factor_workspace_size(int n, int block_size);
+int bbk_factor_device(int n, int block_size, double* a, long long lda,
+                      int* perm, int* pivot_types, int* panel_end,
+                      int update_mode, void* workspace,
+                      size_t workspace_bytes, void* stream);
+/* Same, without the final wait: the device status (a bbk_status) is
+ * written to *status_device when the stream reaches it.  Capturable in a
+ * CUDA graph when `workspace` is given. */
+int bbk_factor_device_async(int n, int block_size, double* a, long long lda,
+                            int* perm, int* pivot_types, int* panel_end,
+                            int update_mode, void* workspace,
+                            size_t workspace_bytes, int* status_device,
+                            void* stream);
+/* Host variant: a (n x lda, in/out), perm, pivot_types, panel_end are host
+ * memory.  Copies in, factors on the current device, copies out. */
+int bbk_factor_host(int n, int block_size, double* a, long long lda,
+                    int* perm, int* pivot_types, int* panel_end,
+                    int update_mode);
+
+/* ---- solve with compact factors (no reference counterpart: the reference
+ * exposes no solve; semantics follow its compact-storage reading rules,
+ * tests/block_ldlt_large_stress_test.cc:160-194) --------------------------
+ * Solves A X = B for nrhs right-hand sides stored column after column
+ * (b[c*ldb + i]); X overwrites B.  A zero 1x1 pivot yields a zero component
+ * (the reference zeroes that column of L); a singular 2x2 pivot divides by
+ * zero. */
+size_t bbk_solve_workspace_size(int n, int nrhs);
+int bbk_solve_device(int n, const double* factors, long long ldf,
+                     const int* perm, const int* pivot_types, int nrhs,
+                     double* b, long long ldb, void* workspace,
+                     size_t workspace_bytes, void* stream);
+int bbk_solve_host(int n, const double* factors, long long ldf,
+                   const int* perm, const int* pivot_types, int nrhs,
+                   double* b, long long ldb);
+
+/* ---- factor + solve in one call, host buffers (the end-to-end path) ----
+ * a (in: matrix, out: compact factors), b (in: right-hand sides, out:
+ * solutions). */
+int bbk_factor_solve_host(int n, int block_size, double* a, long long lda,
+                          int* perm, int* pivot_types, int* panel_end,
+                          int nrhs, double* b, long long ldb, int update_mode);
+
+/* ---- reconstruction (reference ReconstructOriginal,
+ * src/block_ldlt_decomposition.cc:61-78) --------------------------------
+ * out (n x ldo row-major, full) = P^T L D L^T P from compact factors.
+ * Device pointers. */
+int bbk_reconstruct_device(int n, const double* factors, long long ldf,
+                           const int* perm, const int* pivot_types,
+                           double* out, long long ldo, void* stream);
+
+/* ---- the reference's kernel boundary (include/kernels.h:6-23,
+ * src/kernels.cc:11-91), device pointers, element strides -------------- */
+/* kernels::ScaleOneByOnePivot: dst[i*ds] = src[i*ss] / pivot, or 0 when
+ * pivot == 0. */
+int bbk_scale_one_by_one(int count, double pivot, const double* source,
+                         int source_stride, double* destination,
+                         int destination_stride, void* stream);
+/* kernels::ScaleTwoByTwoPivot: [d1; d2] = inv([[a, b], [b, c]]) [s1; s2],
+ * or zeros when the determinant is 0. */
+int bbk_scale_two_by_two(int count, double a, double b, double c,
+                         const double* first_source, int first_source_stride,
+                         const double* second_source, int second_source_stride,
+                         double* first_destination,
+                         int first_destination_stride,
+                         double* second_destination,
+                         int second_destination_stride, void* stream);
+/* kernels::UpdateTrailingBlock: target[rows x cols] -= left^T ws, with left
+ * inner x rows and ws inner x cols, all row-major with the given strides. */
+int bbk_update_trailing_block(int rows, int cols, int inner_dim,
+                              const double* left_panel, int left_panel_stride,
+                              const double* workspace_panel,
+                              int workspace_panel_stride, double* target,
+                              int target_stride, int update_mode,
+                              void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BBK_LDLT_H_ */

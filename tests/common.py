@@ -1,0 +1,86 @@
+"""Shared helpers for the tests (inputs and fixtures, no product code)."""
+import hashlib
+import json
+import os
+
+import numpy as np
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+# tests/block_ldlt_decomposition_test.cc:421-450 of the reference: the golden
+# 4x4 input, its expected compact upper factor and pivot types.
+GOLDEN_4x4 = np.array([[6.0, 12.0, 3.0, -6.0], [12.0, -8.0, -13.0, 4.0],
+                       [3.0, -13.0, -1.0, 1.0], [-6.0, 4.0, 1.0, 6.0]])
+GOLDEN_4x4_COMPACT = np.array([[6.0, 12.0, -0.6875, 0.0],
+                               [0.0, -8.0, 0.59375, -0.5],
+                               [0.0, 0.0, 8.78125, -0.6263345195729537],
+                               [0.0, 0.0, 0.0, 4.555160142348754]])
+GOLDEN_4x4_PIVOTS = [2, -2, 1, 1]
+# tests/block_ldlt_decomposition_test.cc:476-499: the fixed matrices
+FIXED = [GOLDEN_4x4,
+         np.array([[0, 1, 0, 0], [1, 0, 0, 0], [0, 0, 0, 1], [0, 0, 1, 0]], float),
+         np.diag([2.0, -3.0, 0.0, 5.0])]
+TOLERANCE = 1e-10  # tests/block_ldlt_decomposition_test.cc:31
+
+
+def uniform_symmetric(n: int, seed: int) -> np.ndarray:
+    """Entries i.i.d. uniform[-1, 1] from numpy PCG64, upper triangle mirrored."""
+    rng = np.random.default_rng(seed)
+    u = rng.uniform(-1.0, 1.0, size=(n, n))
+    return np.triu(u) + np.triu(u, 1).T
+
+
+def relative_error(actual, expected) -> float:
+    """||actual - expected||_F / max(||expected||_F, 1), the reference's metric."""
+    return float(np.linalg.norm(actual - expected) / max(np.linalg.norm(expected), 1.0))
+
+
+def upper_hash(f: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(np.triu(f)).tobytes()).hexdigest()
+
+
+def load_small_cases():
+    z = np.load(os.path.join(GOLDEN, "ref_cases.npz"))
+    out = []
+    for name in z["names"]:
+        name = str(name)
+        out.append(dict(name=name, a=z[f"{name}__a"], f=z[f"{name}__f"], perm=z[f"{name}__perm"],
+                        pt=z[f"{name}__pt"], ends=z[f"{name}__ends"], b=int(z[f"{name}__b"][0])))
+    return out
+
+
+def load_large_cases():
+    with open(os.path.join(GOLDEN, "ref_large.json")) as fh:
+        return json.load(fh)
+
+
+def reconstruct(f: np.ndarray, perm: np.ndarray, pt: np.ndarray) -> np.ndarray:
+    """P^T L D L^T P in numpy from compact factors (test-side checker)."""
+    n = f.shape[0]
+    L = np.eye(n)
+    D = np.zeros((n, n))
+    for k in range(n):
+        D[k, k] = f[k, k]
+        for i in range(k + 1, n):
+            if pt[k] == 2 and i == k + 1:
+                D[k, k + 1] = D[k + 1, k] = f[k, k + 1]
+            else:
+                L[i, k] = f[k, i]
+    m = L @ D @ L.T
+    out = np.zeros_like(m)
+    out[np.ix_(perm, perm)] = m
+    return out
+
+
+def kkt_matrix(n: int, h: int, seed: int, ridge: float = 1e-2) -> np.ndarray:
+    """Saddle-point [[H, B^T], [B, 0]]: H = G G^T / h + ridge I (G Gaussian
+    h x h), B Gaussian (n-h) x h, zero (2,2) block."""
+    rng = np.random.default_rng(seed)
+    g = rng.standard_normal((h, h))
+    hm = g @ g.T / h + ridge * np.eye(h)
+    bm = rng.standard_normal((n - h, h))
+    a = np.zeros((n, n))
+    a[:h, :h] = hm
+    a[h:, :h] = bm
+    a[:h, h:] = bm.T
+    return a

@@ -1,0 +1,98 @@
+"""Regenerate the golden fixtures in this folder from the reference itself.
+
+Runs in the build container only (it needs oracle/_ref/libbbk_ref.so, compiled
+from the reference's own sources by oracle/Makefile).  Each case stores the
+reference's outputs for an input that the tests can regenerate exactly:
+
+* ``ref_cases.npz``: small cases (the reference tests' libstdc++ generator,
+  the golden 4x4, the fixed matrices): full compact upper factor, perm, pivot
+  types, panel ends;
+* ``ref_large.json``: larger cases (seeded uniform[-1,1] inputs from numpy's
+  PCG64): perm and pivot types in full, plus a SHA-256 of the compact upper
+  factor's bytes so a bitwise match can be checked without storing it.
+
+Usage: python tests/golden/make_golden.py
+"""
+import hashlib
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+from oracle.oracle import Port, Reference  # noqa: E402
+
+GOLDEN_4x4 = [[6.0, 12.0, 3.0, -6.0], [12.0, -8.0, -13.0, 4.0],
+              [3.0, -13.0, -1.0, 1.0], [-6.0, 4.0, 1.0, 6.0]]
+FIXED = [GOLDEN_4x4,
+         [[0, 1, 0, 0], [1, 0, 0, 0], [0, 0, 0, 1], [0, 0, 1, 0]],
+         [[2, 0, 0, 0], [0, -3, 0, 0], [0, 0, 0, 0], [0, 0, 0, 5]]]
+
+
+def uniform_symmetric(n: int, seed: int) -> np.ndarray:
+    """Entries i.i.d. uniform[-1, 1], upper triangle read and mirrored."""
+    rng = np.random.default_rng(seed)
+    u = rng.uniform(-1.0, 1.0, size=(n, n))
+    return np.triu(u) + np.triu(u, 1).T
+
+
+def upper_hash(f: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(np.triu(f)).tobytes()).hexdigest()
+
+
+def small_cases(port: Port):
+    cases = []
+    for ci, m in enumerate(FIXED):
+        for b in range(1, 5):
+            cases.append((f"fixed{ci}_b{b}", np.array(m, float), b))
+    for n in (5, 8, 13, 16):
+        for b in sorted({1, 2, 3, n // 2, n}):
+            seed = 10000 * n + 100 * b
+            cases.append((f"rand_n{n}_b{b}", port.random_symmetric(n, seed), b))
+    for n, b, scale in ((33, 8, 1e-6), (33, 5, 1e6), (64, 16, 1.0), (64, 21, 1e-12)):
+        seed = 910000 + 10000 * n + 100 * b
+        cases.append((f"stress_n{n}_b{b}_s{scale:g}", port.random_symmetric(n, seed, scale), b))
+    for n, b in ((40, 7), (48, 16)):
+        cases.append((f"uniform_n{n}_b{b}", uniform_symmetric(n, 1000 + n), b))
+    return cases
+
+
+def main():
+    port, ref = Port(), Reference()
+    out = {}
+    names = []
+    for name, a, b in small_cases(port):
+        r = ref.factor(a, b)
+        n = a.shape[0]
+        ends = np.array([g[0] + g[1] for g in
+                         (r.geometry[bc + bc * (bc + 1) // 2] for bc in range((n + b - 1) // b))],
+                        np.int32)
+        out[f"{name}__a"] = a
+        out[f"{name}__f"] = np.triu(r.factors)
+        out[f"{name}__perm"] = r.perm
+        out[f"{name}__pt"] = r.pivot_types
+        out[f"{name}__ends"] = ends
+        out[f"{name}__b"] = np.array([b], np.int32)
+        names.append(name)
+    out["names"] = np.array(names)
+    np.savez_compressed(os.path.join(HERE, "ref_cases.npz"), **out)
+
+    large = []
+    for n, b, seed in ((500, 64, 500), (2000, 64, 12345)):
+        a = uniform_symmetric(n, seed)
+        r = ref.factor(a, b)
+        nbk = (n + b - 1) // b
+        ends = [int(g[0] + g[1]) for g in (r.geometry[bc + bc * (bc + 1) // 2] for bc in range(nbk))]
+        large.append({"n": n, "block_size": b, "seed": seed, "generator": "numpy-pcg64-uniform[-1,1]",
+                      "perm": r.perm.tolist(), "pivot_types": r.pivot_types.tolist(),
+                      "panel_end": ends, "upper_sha256": upper_hash(r.factors),
+                      "upper_sum": float(np.triu(r.factors).sum())})
+    with open(os.path.join(HERE, "ref_large.json"), "w") as fh:
+        json.dump(large, fh)
+    print(f"wrote {len(names)} small cases and {len(large)} large cases")
+
+
+if __name__ == "__main__":
+    main()

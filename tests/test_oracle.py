@@ -1,0 +1,90 @@
+"""CPU: the oracle against the reference's golden vectors and the reference.
+
+The oracle is the checker for every GPU parity test, so it is pinned first:
+bitwise against the reference's own golden compact factor, against fixtures
+produced by the reference library (tests/golden/make_golden.py), and, where
+the reference was compiled here, against the reference directly.
+"""
+import numpy as np
+import pytest
+
+from common import (FIXED, GOLDEN_4x4, GOLDEN_4x4_COMPACT, GOLDEN_4x4_PIVOTS, TOLERANCE,
+                    load_large_cases, load_small_cases, reconstruct, relative_error, uniform_symmetric,
+                    upper_hash)
+
+
+def test_golden_compact_storage(port):
+    # tests/block_ldlt_decomposition_test.cc:421-450
+    f = port.factor(GOLDEN_4x4, 2)
+    assert relative_error(np.triu(f.factors), GOLDEN_4x4_COMPACT) < TOLERANCE
+    assert f.pivot_types.tolist() == GOLDEN_4x4_PIVOTS
+
+
+def test_kernel_shapes(port):
+    # tests/block_ldlt_decomposition_test.cc:367-385
+    d0 = port.scale_one_by_one(2.0, [2.0, 4.0, 6.0])
+    assert d0[0] == 1.0 and d0[2] == 3.0
+    d1, d2 = port.scale_two_by_two(2.0, 1.0, 3.0, [1.0, 2.0], [3.0, 4.0])
+    assert abs(d1[0]) < 1e-14 and abs(d2[0] - 1.0) < 1e-14
+
+
+@pytest.mark.parametrize("ci", range(3))
+@pytest.mark.parametrize("b", range(1, 5))
+def test_fixed_factorizations(port, ci, b):
+    # tests/block_ldlt_decomposition_test.cc:476-508
+    a = FIXED[ci]
+    f = port.factor(a, b)
+    assert relative_error(port.reconstruct(f), a) < TOLERANCE
+    assert relative_error(reconstruct(f.factors, f.perm, f.pivot_types), a) < TOLERANCE
+
+
+def test_small_cases_bitwise_vs_fixtures(port):
+    for c in load_small_cases():
+        f = port.factor(c["a"], c["b"])
+        assert np.array_equal(np.triu(f.factors), c["f"], equal_nan=True), c["name"]
+        assert np.array_equal(f.perm, c["perm"]), c["name"]
+        assert np.array_equal(f.pivot_types, c["pt"]), c["name"]
+        assert np.array_equal(f.panel_end, c["ends"]), c["name"]
+
+
+def test_large_case_bitwise_vs_fixture(port):
+    c = [c for c in load_large_cases() if c["n"] == 500][0]
+    f = port.factor(uniform_symmetric(c["n"], c["seed"]), c["block_size"])
+    assert f.perm.tolist() == c["perm"]
+    assert f.pivot_types.tolist() == c["pivot_types"]
+    assert f.panel_end.tolist() == c["panel_end"]
+    assert upper_hash(f.factors) == c["upper_sha256"]
+
+
+def test_random_factorizations_vs_reference(port, reference):
+    # tests/block_ldlt_decomposition_test.cc:510-522 (sizes 3..16, every block size)
+    for n in range(3, 17):
+        for b in range(1, n + 1):
+            for s in range(2):
+                a = port.random_symmetric(n, 10000 * n + 100 * b + s)
+                fp, fr = port.factor(a, b), reference.factor(a, b)
+                assert np.array_equal(np.triu(fp.factors), np.triu(fr.factors)), (n, b, s)
+                assert np.array_equal(fp.perm, fr.perm) and np.array_equal(fp.pivot_types, fr.pivot_types)
+
+
+def test_scale_sweep_vs_reference(port, reference):
+    # tests/block_ldlt_decomposition_test.cc:40-99, 524-534 (a subset)
+    scales = [1e-12, 1e-9, 1e-6, 1e-3, 1.0, 1e3, 1e6, 1e9, 1e12]
+    for n in (5, 20, 50):
+        for b in (1, 3, 8, 21):
+            if b > n:
+                continue
+            for si, sc in enumerate(scales):
+                a = port.random_symmetric(n, 910000 + 10000 * n + 100 * b + 10 * si, sc)
+                fp, fr = port.factor(a, b), reference.factor(a, b)
+                assert np.array_equal(np.triu(fp.factors), np.triu(fr.factors)), (n, b, sc)
+                assert relative_error(port.reconstruct(fp), a) < TOLERANCE
+
+
+def test_solve_restatement(port):
+    a = uniform_symmetric(60, 3)
+    f = port.factor(a, 8)
+    rng = np.random.default_rng(0)
+    b = rng.standard_normal((60, 3))
+    x = port.solve(f, b)
+    assert np.linalg.norm(a @ x - b) / np.linalg.norm(b) < 1e-10
