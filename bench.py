@@ -1,0 +1,491 @@
+#!/usr/bin/env python
+"""LDL^T solve benchmark on B200.
+
+Workload (default): plain FP64 blocked Bunch-Kaufman LDL^T factorization plus
+one solve of the saddle-point KKT matrix [[H, B^T], [B, 0]], n = 10000 with
+H 8000 x 8000 = G G^T / 8000 + 1e-2 I (G Gaussian), B 2000 x 8000 Gaussian,
+block size 128, one right-hand side b ~ N(0, 1).  Seeded synthetic inputs.
+
+metric: GFLOP/s = (n^3 / 3) / (time of factorization + solve), whole job.
+
+Arms:
+  (default)          this library on the GPU(s); one process per GPU under
+                     torchrun, replicas only (every rank factors its own copy).
+  --impl reference   the reference's own CPU implementation (compiled from its
+                     sources into oracle/_ref) on the host cores, a bounded
+                     sample of the workload per step.
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import datetime
+import io
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "LDL^T solve GFLOP/s: FP64 vs FP32/BF16+IR at <=1e-12 bwd err; batched mats/s"
+UNIT = "GFLOP/s"
+MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=10000)
+    ap.add_argument("--h", type=int, default=None, help="H block order (default 0.8 n)")
+    ap.add_argument("--block", type=int, default=128)
+    ap.add_argument("--nrhs", type=int, default=1)
+    ap.add_argument("--mode", default="fp64", choices=["fp64", "fp64_ordered", "fp32"])
+    ap.add_argument("--seed", type=int, default=20240)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU baseline sample time")
+    return ap.parse_args()
+
+
+def flops_ldlt(n: int) -> float:
+    return n ** 3 / 3.0
+
+
+def workload_config(args, n_used=None) -> dict:
+    n = args.n if n_used is None else n_used
+    h = args.h if args.h is not None else int(round(0.8 * args.n))
+    return {
+        "workload": f"plain FP64 blocked Bunch-Kaufman LDL^T factor + solve, KKT n={n} "
+                    f"(H {h if n_used is None else int(round(0.8 * n))} SPD, B Gaussian, zero (2,2) block), "
+                    f"block {args.block}, {args.nrhs} RHS",
+        "n": n, "block_size": args.block, "nrhs": args.nrhs, "update": args.mode,
+        "l2": "inputs larger than L2 (the n x n FP64 matrix); the input is restored by a device "
+              "copy inside each timed step",
+    }
+
+
+# ---------------------------------------------------------------------------
+# clocks sampling (nvidia-smi during the timed region)
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(prefix="bbk_clocks_", suffix=".csv")
+            os.close(fd)
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=self.out, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.out.close()
+        rows = []
+        with open(self.path) as fh:
+            for r in csv.reader(fh):
+                if len(r) >= 9:
+                    rows.append([x.strip() for x in r])
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        loaded = [s for s in sm if s > 0.5 * max(sm)] if sm else []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# inputs
+# ---------------------------------------------------------------------------
+def kkt_device(n: int, h: int, seed: int, device):
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    gm = torch.randn(h, h, generator=g, dtype=torch.float64, device=device)
+    a = torch.zeros(n, n, dtype=torch.float64, device=device)
+    a[:h, :h] = gm @ gm.T / h
+    a[:h, :h] += 1e-2 * torch.eye(h, dtype=torch.float64, device=device)
+    del gm
+    bm = torch.randn(n - h, h, generator=g, dtype=torch.float64, device=device)
+    a[h:, :h] = bm
+    a[:h, h:] = bm.T
+    rhs = torch.randn(n, generator=g, dtype=torch.float64, device=device)
+    return a, rhs
+
+
+def kkt_host(n: int, h: int, seed: int):
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    g = rng.standard_normal((h, h))
+    a = np.zeros((n, n))
+    a[:h, :h] = g @ g.T / h + 1e-2 * np.eye(h)
+    bm = rng.standard_normal((n - h, h))
+    a[h:, :h] = bm
+    a[:h, h:] = bm.T
+    return a
+
+
+def measure_dgemm_tflops(device) -> float:
+    import torch
+    n = 8192
+    x = torch.randn(n, n, dtype=torch.float64, device=device)
+    y = torch.randn(n, n, dtype=torch.float64, device=device)
+    for _ in range(2):
+        z = x @ y
+    torch.cuda.synchronize()
+    best = float("inf")
+    for _ in range(3):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        z = x @ y
+        e.record()
+        torch.cuda.synchronize()
+        best = min(best, s.elapsed_time(e) / 1e3)
+    del x, y, z
+    return 2 * n ** 3 / best / 1e12
+
+
+def measured_hbm_gbs():
+    try:
+        with open(MEASURED_PEAKS) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (measured)"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback 6.65 TB/s"
+
+
+# ---------------------------------------------------------------------------
+# algorithmic work per kernel class
+# ---------------------------------------------------------------------------
+def update_flops(n: int, panel_end) -> float:
+    f, k0 = 0.0, 0
+    for e in panel_end:
+        kb, m = e - k0, n - e
+        if m > 0:
+            f += 2.0 * kb * m * (m + 1) / 2.0
+        k0 = e
+    return f
+
+
+def panel_bytes(n: int, panel_end) -> float:
+    """Lower bound on the panel kernels' traffic: per pivot p (local index lp)
+    the row update reads lp workspace rows and the matrix row over n - p
+    columns and writes the workspace row and the factor row."""
+    b, k0 = 0.0, 0
+    for e in panel_end:
+        for p in range(k0, e):
+            b += 8.0 * (n - p) * ((p - k0) + 3)
+        k0 = e
+    return b
+
+
+# ---------------------------------------------------------------------------
+# this library
+# ---------------------------------------------------------------------------
+def run_b200(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import blockedbunchkaufmanldlt_b200 as bbk
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    n, blk, nrhs = args.n, args.block, args.nrhs
+    h = args.h if args.h is not None else int(round(0.8 * n))
+    a0, b0 = kkt_device(n, h, args.seed, dev)
+    rhs0 = b0.repeat(nrhs, 1).contiguous() if nrhs > 1 else b0.reshape(1, n).contiguous()
+    dgemm = measure_dgemm_tflops(dev)
+    hbm, hbm_src = measured_hbm_gbs()
+
+    work = torch.empty_like(a0)
+    x = torch.empty_like(rhs0)
+    ws_f = torch.empty(bbk.factor_workspace_size(n, blk), dtype=torch.uint8, device=dev)
+    ws_s = torch.empty(bbk.solve_workspace_size(n, nrhs), dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+    L = bbk.lib()
+    import ctypes
+    nb = (n + blk - 1) // blk
+    perm = torch.empty(n, dtype=torch.int32, device=dev)
+    pt = torch.empty(n, dtype=torch.int32, device=dev)
+    pe = torch.empty(nb, dtype=torch.int32, device=dev)
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
+    vp = ctypes.c_void_p
+    sp = vp(stream.cuda_stream)
+    mode = bbk.UPDATE_MODES[args.mode]
+
+    def step():
+        work.copy_(a0)
+        bbk.check(L.bbk_factor_device_async(n, blk, vp(work.data_ptr()), n, vp(perm.data_ptr()),
+                                            vp(pt.data_ptr()), vp(pe.data_ptr()), mode, vp(ws_f.data_ptr()),
+                                            ws_f.numel(), vp(status.data_ptr()), sp))
+        x.copy_(rhs0)
+        bbk.check(L.bbk_solve_device(n, vp(work.data_ptr()), n, vp(perm.data_ptr()), vp(pt.data_ptr()),
+                                     nrhs, vp(x.data_ptr()), n, vp(ws_s.data_ptr()), ws_s.numel(), sp))
+
+    for _ in range(max(args.warmup, 0)):
+        step()
+    torch.cuda.synchronize()
+    if int(status.item()) != 0:
+        raise RuntimeError(f"device status {int(status.item())}")
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    barrier()
+    torch.cuda.synchronize()
+    launches0 = bbk.kernel_launch_count()
+    bbk.profile_begin()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(args.steps):
+        step()
+    ev1.record()
+    torch.cuda.synchronize()
+    barrier()
+    prof = bbk.profile_end()
+    launches = bbk.kernel_launch_count() - launches0
+    clocks = sampler.stop()
+    ms = max_over_ranks(ev0.elapsed_time(ev1))
+    ms_step = ms / args.steps
+    value = world * flops_ldlt(n) / (ms_step / 1e3) / 1e9
+
+    # accuracy of the last step: backward error of the solve (FP64, on device)
+    asym = a0
+    r = rhs0.T - asym @ x.T
+    berr = float((r.abs().amax() / (asym.abs().sum(1).amax() * x.abs().amax() + rhs0.abs().amax())).item())
+    pe_h = pe.cpu().numpy().tolist()
+    pt_h = pt.cpu().numpy()
+    n1, n2 = int((pt_h == 1).sum()), int((pt_h == 2).sum())
+    shifts = sum(1 for P, e in enumerate(pe_h) if e < min((P + 1) * blk, n))
+
+    # per-kernel roofline from the live profile
+    upd_flops = update_flops(n, pe_h) * args.steps
+    pan_bytes = panel_bytes(n, pe_h) * args.steps
+    kernels = {}
+    if prof["update"]["ms"] > 0:
+        kernels["trailing_update"] = {
+            "bound": "tensor", "achieved": upd_flops / (prof["update"]["ms"] / 1e3) / 1e12, "unit": "TFLOP/s",
+            "peak": dgemm, "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor peak)",
+            "ms": prof["update"]["ms"], "launches": prof["update"]["launches"]}
+        kernels["trailing_update"]["frac"] = kernels["trailing_update"]["achieved"] / dgemm
+    if prof["panel"]["ms"] > 0:
+        kernels["panel"] = {
+            "bound": "hbm", "achieved": pan_bytes / (prof["panel"]["ms"] / 1e3) / 1e9, "unit": "GB/s",
+            "peak": hbm, "peak_source": hbm_src, "ms": prof["panel"]["ms"], "launches": prof["panel"]["launches"]}
+        kernels["panel"]["frac"] = kernels["panel"]["achieved"] / hbm
+    for k in ("finalize", "solve", "init"):
+        kernels[k] = {"ms": prof[k]["ms"], "launches": prof[k]["launches"]}
+    total_prof = sum(prof[k]["ms"] for k in prof)
+    for k, v in kernels.items():
+        v["share"] = (v["ms"] / total_prof) if total_prof > 0 else None
+    dom = max(("trailing_update", "panel"), key=lambda k: kernels.get(k, {}).get("ms", 0.0))
+    dk = kernels[dom]
+    traffic = None
+    traffic_path = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(traffic_path):
+        try:
+            with open(traffic_path) as fh:
+                traffic = json.load(fh).get(dom)
+        except (OSError, ValueError):
+            traffic = None
+    roofline = {"kernel": dom, "bound": dk["bound"], "achieved": dk["achieved"], "peak": dk["peak"],
+                "unit": dk["unit"], "frac": dk["frac"], "traffic": traffic, "peak_source": dk["peak_source"]}
+
+    # end to end through the host-buffer C ABI (pinned host memory)
+    e2e = None
+    if not args.no_e2e:
+        ha = a0.cpu().pin_memory()
+        hb = rhs0.cpu().pin_memory()
+        hwork = torch.empty_like(ha).pin_memory()
+        hx = torch.empty_like(hb).pin_memory()
+        hperm = torch.empty(n, dtype=torch.int32).pin_memory()
+        hpt = torch.empty(n, dtype=torch.int32).pin_memory()
+        hpe = torch.empty(nb, dtype=torch.int32).pin_memory()
+
+        def restore():
+            hwork.copy_(ha)
+            hx.copy_(hb)
+
+        def e2e_call():
+            bbk.check(L.bbk_factor_solve_host(n, blk, vp(hwork.data_ptr()), n, vp(hperm.data_ptr()),
+                                              vp(hpt.data_ptr()), vp(hpe.data_ptr()), nrhs, vp(hx.data_ptr()),
+                                              n, mode))
+
+        restore()
+        e2e_call()
+        k_e2e = max(1, min(args.steps, 5))
+        tot_ms = 0.0
+        for _ in range(k_e2e):
+            restore()  # the caller's input is restored outside the timed call
+            barrier()
+            torch.cuda.synchronize()
+            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0 = time.perf_counter()
+            s0.record()
+            e2e_call()  # synchronous: H2D, factor, solve, D2H
+            s1.record()
+            torch.cuda.synchronize()
+            wall = (time.perf_counter() - t0) * 1e3
+            tot_ms += max(s0.elapsed_time(s1), wall)
+        ems = max_over_ranks(tot_ms) / k_e2e
+        h2d = n * n * 8 + nrhs * n * 8
+        d2h = n * n * 8 + nrhs * n * 8 + 4 * (2 * n + nb)
+        e2e = {"value": world * flops_ldlt(n) / (ems / 1e3) / 1e9, "unit": UNIT, "ms_per_step": ems,
+               "steps": k_e2e, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "api": "bbk_factor_solve_host (host buffers, pinned): H2D of matrix and rhs, factor, "
+                      "solve, D2H of compact factors, pivots and solution, inside each timed step"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample(args, target_s=args.cpu_seconds)
+
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.mode != "fp32" else "f64+f32-update",
+        "data": "synthetic: seeded KKT saddle-point matrix (torch Gaussian generators on the device)",
+        "config": dict(workload_config(args), parallelism=f"replicas x{world} (one matrix per GPU)",
+                       seed=args.seed),
+        "e2e": e2e, "roofline": roofline, "kernels": kernels, "cpu_baseline": cpu,
+        "clocks": clocks, "gpu_launches": launches,
+        "accuracy": {"backward_error": berr, "pivots_1x1": n1, "pivots_2x2": n2, "boundary_shifts": shifts},
+        "fp64_dgemm_tflops": dgemm,
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# CPU: the reference (oracle/_ref) on the host cores
+# ---------------------------------------------------------------------------
+def _reference_lib():
+    os.environ.setdefault("OMP_PROC_BIND", "close")
+    from oracle.oracle import Port, Reference
+    if Reference.available():
+        return Reference(), "reference"
+    return Port(), "port"
+
+
+def _cpu_factor(lib, kind, a, blk):
+    if kind == "reference":
+        t0 = time.perf_counter()
+        f = lib.factor(a, blk)
+        return f.seconds if f.seconds else time.perf_counter() - t0
+    t0 = time.perf_counter()
+    lib.factor(a, blk)
+    return time.perf_counter() - t0
+
+
+def _pick_sample_n(lib, kind, args, target_s: float) -> int:
+    n_cal = 1536
+    a = kkt_host(n_cal, int(round(0.8 * n_cal)), args.seed)
+    t = _cpu_factor(lib, kind, a, args.block)
+    rate = flops_ldlt(n_cal) / max(t, 1e-6)
+    n_s = int((3.0 * rate * target_s) ** (1.0 / 3.0))
+    n_s = max(n_cal, min(args.n, (n_s // args.block) * args.block))
+    return n_s
+
+
+def cpu_baseline_sample(args, target_s: float) -> dict:
+    lib, kind = _reference_lib()
+    cores = lib.threads() if kind == "reference" else 1
+    n_s = _pick_sample_n(lib, kind, args, target_s)
+    a = kkt_host(n_s, int(round(0.8 * n_s)), args.seed)
+    t = _cpu_factor(lib, kind, a, args.block)
+    return {"value": flops_ldlt(n_s) / t / 1e9, "unit": UNIT, "cores": cores, "kind": kind,
+            "sample": f"one factorization of a KKT matrix of the same structure at n={n_s} "
+                      f"(H {int(round(0.8 * n_s))}), block {args.block}, ctor + Factorize() timed; "
+                      "the reference has no solve (O(n^2), not timed)",
+            "seconds": t}
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    lib, kind = _reference_lib()
+    cores = lib.threads() if kind == "reference" else 1
+    total_steps = max(1, args.steps) + max(0, args.warmup)
+    per_step = max(2.0, min(30.0, 150.0 / total_steps))
+    n_s = _pick_sample_n(lib, kind, args, per_step)
+    a = kkt_host(n_s, int(round(0.8 * n_s)), args.seed)
+    for _ in range(max(0, args.warmup)):
+        _cpu_factor(lib, kind, a, args.block)
+    times = [_cpu_factor(lib, kind, a, args.block) for _ in range(max(1, args.steps))]
+    tot = sum(times)
+    value = flops_ldlt(n_s) * len(times) / tot / 1e9
+    sample = (f"each step one factorization of a KKT matrix of the same structure at n={n_s} "
+              f"(H {int(round(0.8 * n_s))}), block {args.block}, ctor + Factorize() timed with "
+              f"{cores} OpenMP threads; the reference has no solve")
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": len(times),
+        "warmup": args.warmup, "ms_per_step": tot / len(times) * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "impl": "reference",
+        "data": "synthetic: seeded KKT saddle-point matrix (numpy PCG64)",
+        "config": workload_config(args, n_used=n_s),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -40,12 +40,13 @@ UPDATE_MODES = {"fp64": UPDATE_FP64, "fp64_ordered": UPDATE_FP64_ORDERED, "fp32"
 # Every symbol include/bbk_ldlt.h declares.
 EXPORTS = (
     "bbk_abi_version", "bbk_last_error", "bbk_status_string", "bbk_kernel_launch_count",
-    "bbk_set_wait_timeout_ns", "bbk_probe_bounded_wait", "bbk_factor_workspace_size",
+    "bbk_set_wait_timeout_ns", "bbk_probe_bounded_wait", "bbk_probe_exchange_ns", "bbk_factor_workspace_size",
     "bbk_factor_device", "bbk_factor_device_async", "bbk_factor_host",
     "bbk_solve_workspace_size", "bbk_solve_device", "bbk_solve_host", "bbk_factor_solve_host",
     "bbk_reconstruct_device", "bbk_scale_one_by_one", "bbk_scale_two_by_two",
-    "bbk_update_trailing_block",
+    "bbk_update_trailing_block", "bbk_profile_begin", "bbk_profile_end", "bbk_panel_stats", "bbk_panel_stats_raw",
 )
+PROFILE_CLASSES = ("init", "panel", "finalize", "update", "solve")
 
 
 class BbkError(RuntimeError):
@@ -95,7 +96,12 @@ def lib() -> ctypes.CDLL:
         "bbk_status_string": ([_c_int], ctypes.c_char_p),
         "bbk_kernel_launch_count": ([], ctypes.c_ulonglong),
         "bbk_set_wait_timeout_ns": ([ctypes.c_ulonglong], _c_int),
+        "bbk_profile_begin": ([], _c_int),
+        "bbk_profile_end": ([_vp, _vp], _c_int),
+        "bbk_panel_stats": ([_c_int, _vp], _c_int),
+        "bbk_panel_stats_raw": ([_vp, _c_sz], _c_int),
         "bbk_probe_bounded_wait": ([_c_int, ctypes.c_ulonglong, _vp], _c_int),
+        "bbk_probe_exchange_ns": ([_c_int, _c_int, _vp, _vp], _c_int),
         "bbk_factor_workspace_size": ([_c_int, _c_int], _c_sz),
         "bbk_factor_device": ([_c_int, _c_int, _vp, _c_ll, _vp, _vp, _vp, _c_int, _vp, _c_sz, _vp], _c_int),
         "bbk_factor_device_async": ([_c_int, _c_int, _vp, _c_ll, _vp, _vp, _vp, _c_int, _vp, _c_sz,
@@ -129,6 +135,35 @@ def check(status: int) -> None:
 
 def kernel_launch_count() -> int:
     return int(lib().bbk_kernel_launch_count())
+
+
+def profile_begin() -> None:
+    check(lib().bbk_profile_begin())
+
+
+def profile_end() -> dict:
+    """Per-class device milliseconds and launch counts since profile_begin()."""
+    ms = (ctypes.c_double * 5)()
+    cnt = (ctypes.c_longlong * 5)()
+    check(lib().bbk_profile_end(ctypes.cast(ms, ctypes.c_void_p), ctypes.cast(cnt, ctypes.c_void_p)))
+    return {k: {"ms": ms[i], "launches": cnt[i]} for i, k in enumerate(PROFILE_CLASSES)}
+
+
+PANEL_PHASES = ("row_update", "exchange_1", "candidate", "exchange_2", "swap_scale")
+
+
+def panel_stats(enable: bool):
+    """Arm (True) or read and disarm (False) the panel phase timers."""
+    out = (ctypes.c_ulonglong * 10)()
+    check(lib().bbk_panel_stats(1 if enable else 0, ctypes.cast(out, ctypes.c_void_p)))
+    if enable:
+        return None
+    d = {k: out[i] / 1e6 for i, k in enumerate(PANEL_PHASES)}  # ms
+    d["pivots"] = int(out[5])
+    d["candidates"] = int(out[6])
+    d["exchange_wait_for_last_ms"] = out[7] / 1e6
+    d["exchange_propagation_ms"] = out[8] / 1e6
+    return d
 
 
 def set_wait_timeout_ns(ns: int) -> None:
@@ -226,6 +261,13 @@ def probe_bounded_wait(ctas: int, timeout_ns: int, stream=None) -> int:
     """Run the bounded-wait probe; returns the bbk_status (BBK_ERR_TIMEOUT
     when the device-side wait bound works)."""
     return int(lib().bbk_probe_bounded_wait(ctas, timeout_ns, _stream_ptr(stream)))
+
+
+def probe_exchange_ns(ctas: int, iters: int = 2000, stream=None) -> float:
+    """Mean device nanoseconds of one grid exchange on `ctas` blocks."""
+    out = ctypes.c_double(0.0)
+    check(lib().bbk_probe_exchange_ns(ctas, iters, ctypes.byref(out), _stream_ptr(stream)))
+    return out.value
 
 
 # ---------------------------------------------------------------------------

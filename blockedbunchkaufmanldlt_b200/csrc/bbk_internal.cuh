@@ -98,14 +98,16 @@ __device__ __forceinline__ unsigned long long tag_word(unsigned tag, unsigned v)
 namespace bbk {
 struct FactorPlan;
 int panel_grid_size(int n);
+int panel_max_n();
 int launch_init(int n, int* perm, int* pivot_types, DeviceState* st,
                 unsigned long long* slots, size_t slot_words, cudaStream_t s);
 int launch_panel(const FactorPlan& plan, int panel, cudaStream_t s);
 int launch_finalize(const FactorPlan& plan, int panel, cudaStream_t s);
 int launch_update(const FactorPlan& plan, int panel, cudaStream_t s);
 int launch_status_copy(const DeviceState* st, int* status_out, cudaStream_t s);
-int launch_probe_wait(int ctas, unsigned long long timeout_ns, DeviceState* st,
-                      unsigned long long* slots, cudaStream_t s);
+int launch_probe_wait(int ctas, int nslots, int iters, unsigned long long timeout_ns,
+                      DeviceState* st, unsigned long long* slots, unsigned long long* stats,
+                      cudaStream_t s);
 int launch_update_block(int rows, int cols, int inner, const double* left, int ls,
                         const double* ws, int wss, double* target, int ts, int mode,
                         cudaStream_t s);
@@ -145,5 +147,6 @@ struct FactorPlan {
   DeviceState* state = nullptr;
   int grid = 0;              // CTAs of the panel kernel
   unsigned long long timeout_ns = 0;
+  unsigned long long* stats = nullptr;  // optional per-phase panel timing
 };
 }  // namespace bbk

@@ -1,6 +1,8 @@
 // extern "C" entry points of libbbk_b200 (declared in include/bbk_ldlt.h).
 #include <atomic>
 #include <cstdarg>
+#include <mutex>
+#include <vector>
 #include <cstdio>
 #include <cstring>
 
@@ -17,6 +19,41 @@ constexpr int kMaxPanelGrid = 1024;
 constexpr size_t kAlign = 256;
 
 int g_sm_count[64] = {0};
+
+// Optional per-class device timing (bbk_profile_begin/end).
+enum ProfClass { kProfInit = 0, kProfPanel, kProfFinalize, kProfUpdate, kProfSolve, kProfClasses };
+struct ProfRecord {
+  int cls;
+  cudaEvent_t start, stop;
+};
+std::mutex g_prof_mu;
+bool g_prof_on = false;
+std::vector<ProfRecord> g_prof;
+std::vector<cudaEvent_t> g_event_pool;
+
+cudaEvent_t pool_event() {
+  if (!g_event_pool.empty()) {
+    cudaEvent_t e = g_event_pool.back();
+    g_event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// Runs `launch` between two events on stream s when profiling is on.
+template <typename F>
+int profiled(int cls, cudaStream_t s, F&& launch) {
+  if (!g_prof_on) return launch();
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  ProfRecord r{cls, pool_event(), pool_event()};
+  cudaEventRecord(r.start, s);
+  const int rc = launch();
+  cudaEventRecord(r.stop, s);
+  g_prof.push_back(r);
+  return rc;
+}
 
 int check_device() {
   int dev = 0;
@@ -54,10 +91,15 @@ size_t carve_factor(FactorPlan& plan, char* base) {
   plan.w = c.take<double>(static_cast<size_t>(b + 2) * npad);
   plan.ucm = c.take<double>(static_cast<size_t>(npad) * plan.ldu);
   plan.uout = c.take<double>(static_cast<size_t>(b + 2) * plan.ldu);
-  plan.wc = c.take<double>(static_cast<size_t>(npad));
+  // candidate column (n) followed by the interchange staging area
+  plan.wc = c.take<double>(static_cast<size_t>(npad) + 2 * align_up(static_cast<size_t>(b) + 4, 2));
   c.take<int>(4);  // status word for the synchronous entry point
   return c.off;
 }
+
+constexpr size_t kPanelStatsWords = 16 + 1024 + 1024 + 5 * 1024;
+unsigned long long* g_panel_stats = nullptr;  // device counters (diagnostics)
+bool g_panel_stats_on = false;
 
 int validate_factor_args(int n, int block_size, const double* a, long long lda, const int* perm,
                          const int* pivot_types, int mode) {
@@ -104,15 +146,24 @@ int device_sm_count() {
 
 // Enqueue a whole factorization for an already carved plan.
 static int enqueue_factor(FactorPlan& plan, int* status_device, cudaStream_t s) {
-  int rc = launch_init(plan.n, plan.perm, plan.pivot_types, plan.state, plan.slots,
+  int rc = profiled(kProfInit, s, [&] {
+    return launch_init(plan.n, plan.perm, plan.pivot_types, plan.state, plan.slots,
                        2ull * kMaxPanelGrid * kSlotWords, s);
+  });
   if (rc) return rc;
   for (int panel = 0; panel < plan.nb; ++panel) {
-    if ((rc = launch_panel(plan, panel, s))) return rc;
-    if ((rc = launch_finalize(plan, panel, s))) return rc;
-    if ((rc = launch_update(plan, panel, s))) return rc;
+    if ((rc = profiled(kProfPanel, s, [&] { return launch_panel(plan, panel, s); }))) return rc;
+    if ((rc = profiled(kProfFinalize, s, [&] { return launch_finalize(plan, panel, s); }))) return rc;
+    if ((rc = profiled(kProfUpdate, s, [&] { return launch_update(plan, panel, s); }))) return rc;
   }
   return launch_status_copy(plan.state, status_device, s);
+}
+
+static int enqueue_solve(int n, const double* f, long long ldf, const int* perm, const int* pt,
+                         int nrhs, double* b, long long ldb, double* work, cudaStream_t s) {
+  return profiled(kProfSolve, s, [&] {
+    return solve_enqueue(n, f, ldf, perm, pt, nrhs, b, ldb, work, s);
+  });
 }
 
 }  // namespace bbk
@@ -144,6 +195,66 @@ unsigned long long bbk_kernel_launch_count(void) {
   return g_launches.load(std::memory_order_relaxed);
 }
 
+int bbk_profile_begin(void) {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  for (auto& r : g_prof) {
+    g_event_pool.push_back(r.start);
+    g_event_pool.push_back(r.stop);
+  }
+  g_prof.clear();
+  g_prof_on = true;
+  return BBK_OK;
+}
+
+int bbk_profile_end(double* ms, long long* counts) {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  g_prof_on = false;
+  double tot[kProfClasses] = {0};
+  long long cnt[kProfClasses] = {0};
+  int rc = BBK_OK;
+  for (auto& r : g_prof) {
+    cudaError_t err = cudaEventSynchronize(r.stop);
+    float t = 0.f;
+    if (err == cudaSuccess) err = cudaEventElapsedTime(&t, r.start, r.stop);
+    if (err != cudaSuccess && rc == BBK_OK) rc = cuda_error(err, "profile events");
+    tot[r.cls] += t;
+    cnt[r.cls] += 1;
+    g_event_pool.push_back(r.start);
+    g_event_pool.push_back(r.stop);
+  }
+  g_prof.clear();
+  for (int i = 0; i < kProfClasses; ++i) {
+    if (ms) ms[i] = tot[i];
+    if (counts) counts[i] = cnt[i];
+  }
+  return rc;
+}
+
+int bbk_panel_stats(int enable, unsigned long long* out) {
+  int rc = check_device();
+  if (rc) return rc;
+  if (enable) {
+    if (!g_panel_stats) BBK_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&g_panel_stats), kPanelStatsWords * 8));
+    BBK_CUDA_TRY(cudaMemset(g_panel_stats, 0, kPanelStatsWords * 8));
+    g_panel_stats_on = true;
+    return BBK_OK;
+  }
+  g_panel_stats_on = false;
+  if (out && g_panel_stats) {
+    BBK_CUDA_TRY(cudaDeviceSynchronize());
+    BBK_CUDA_TRY(cudaMemcpy(out, g_panel_stats, 10 * 8, cudaMemcpyDeviceToHost));
+  }
+  return BBK_OK;
+}
+
+int bbk_panel_stats_raw(unsigned long long* out, size_t words) {
+  if (!g_panel_stats || !out) return set_error(BBK_ERR_LOGIC, "panel stats never armed");
+  if (words > kPanelStatsWords) words = kPanelStatsWords;
+  BBK_CUDA_TRY(cudaDeviceSynchronize());
+  BBK_CUDA_TRY(cudaMemcpy(out, g_panel_stats, words * 8, cudaMemcpyDeviceToHost));
+  return BBK_OK;
+}
+
 int bbk_set_wait_timeout_ns(unsigned long long timeout_ns) {
   if (timeout_ns == 0) return set_error(BBK_ERR_INVALID_ARGUMENT, "timeout must be positive");
   g_timeout_ns.store(timeout_ns, std::memory_order_relaxed);
@@ -164,6 +275,9 @@ int bbk_factor_device_async(int n, int block_size, double* a, long long lda, int
   int rc = validate_factor_args(n, block_size, a, lda, perm, pivot_types, update_mode);
   if (rc) return rc;
   if ((rc = check_device())) return rc;
+  if (n > panel_max_n())
+    return set_error(BBK_ERR_INVALID_ARGUMENT, "n = %d exceeds this device's panel limit %d", n,
+                     panel_max_n());
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   FactorPlan plan;
   plan.n = n;
@@ -177,6 +291,7 @@ int bbk_factor_device_async(int n, int block_size, double* a, long long lda, int
   plan.panel_end = panel_end;
   plan.grid = panel_grid_size(n);
   plan.timeout_ns = wait_timeout_ns();
+  plan.stats = g_panel_stats_on ? g_panel_stats : nullptr;
   const size_t need = carve_factor(plan, nullptr);
   char* base = static_cast<char*>(workspace);
   bool owned = false;
@@ -266,7 +381,7 @@ int bbk_solve_device(int n, const double* factors, long long ldf, const int* per
     return set_error(BBK_ERR_WORKSPACE, "solve workspace needs %zu bytes, got %zu", need,
                      workspace_bytes);
   }
-  rc = solve_enqueue(n, factors, ldf, perm, pivot_types, nrhs, b, ldb, work, s);
+  rc = enqueue_solve(n, factors, ldf, perm, pivot_types, nrhs, b, ldb, work, s);
   if (owned) cudaFreeAsync(work, s);
   if (rc) return rc;
   BBK_CUDA_TRY(cudaStreamSynchronize(s));
@@ -298,7 +413,7 @@ int bbk_solve_host(int n, const double* factors, long long ldf, const int* perm,
   if (err != cudaSuccess) {
     rc = cuda_error(err, "solve setup");
   } else {
-    rc = solve_enqueue(n, d_f, ldf, d_perm, d_pt, nrhs, d_b, ldb, work, s);
+    rc = enqueue_solve(n, d_f, ldf, d_perm, d_pt, nrhs, d_b, ldb, work, s);
     if (!rc) {
       err = cudaMemcpyAsync(b, d_b, bbytes, cudaMemcpyDeviceToHost, s);
       if (err == cudaSuccess) err = cudaStreamSynchronize(s);
@@ -349,7 +464,7 @@ int bbk_factor_solve_host(int n, int block_size, double* a, long long lda, int* 
   } else {
     rc = bbk_factor_device_async(n, block_size, d_a, lda, d_perm, d_pt, d_pe, update_mode, ws, fws,
                                  d_status, s);
-    if (!rc && nrhs > 0) rc = solve_enqueue(n, d_a, lda, d_perm, d_pt, nrhs, d_b, ldb,
+    if (!rc && nrhs > 0) rc = enqueue_solve(n, d_a, lda, d_perm, d_pt, nrhs, d_b, ldb,
                                             reinterpret_cast<double*>(ws), s);
     if (!rc) {
       err = cudaMemcpyAsync(a, d_a, abytes, cudaMemcpyDeviceToHost, s);
@@ -439,36 +554,60 @@ int bbk_update_trailing_block(int rows, int cols, int inner_dim, const double* l
                              static_cast<cudaStream_t>(stream));
 }
 
-int bbk_probe_bounded_wait(int ctas, unsigned long long timeout_ns, void* stream) {
-  if (ctas <= 0 || ctas > kMaxPanelGrid || timeout_ns == 0)
-    return set_error(BBK_ERR_INVALID_ARGUMENT, "bad probe arguments");
-  int rc = check_device();
-  if (rc) return rc;
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
+static int run_probe(int ctas, int nslots, int iters, unsigned long long timeout_ns,
+                     unsigned long long* elapsed_ns, int* device_status, cudaStream_t s) {
   const size_t slot_words = 2ull * (ctas + 1) * kSlotWords;
-  const size_t bytes = align_up(sizeof(DeviceState), kAlign) + slot_words * 8;
+  const size_t off_slots = align_up(sizeof(DeviceState), kAlign);
+  const size_t off_stats = off_slots + align_up(slot_words * 8, kAlign);
+  const size_t bytes = off_stats + kAlign;
   char* base = nullptr;
   BBK_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&base), bytes, s));
   DeviceState* st = reinterpret_cast<DeviceState*>(base);
-  unsigned long long* slots =
-      reinterpret_cast<unsigned long long*>(base + align_up(sizeof(DeviceState), kAlign));
-  int h_status = BBK_OK;
+  auto* slots = reinterpret_cast<unsigned long long*>(base + off_slots);
+  auto* stats = reinterpret_cast<unsigned long long*>(base + off_stats);
+  int rc = BBK_OK;
   cudaError_t err = cudaMemsetAsync(base, 0, bytes, s);
   if (err != cudaSuccess) {
     rc = cuda_error(err, "cudaMemsetAsync");
   } else {
-    rc = launch_probe_wait(ctas, timeout_ns, st, slots, s);
+    rc = launch_probe_wait(ctas, nslots, iters, timeout_ns, st, slots, stats, s);
     if (!rc) {
-      err = cudaMemcpyAsync(&h_status, &st->status, sizeof(int), cudaMemcpyDeviceToHost, s);
+      err = cudaMemcpyAsync(device_status, &st->status, sizeof(int), cudaMemcpyDeviceToHost, s);
+      if (err == cudaSuccess && elapsed_ns)
+        err = cudaMemcpyAsync(elapsed_ns, stats, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
       if (err == cudaSuccess) err = cudaStreamSynchronize(s);
       if (err != cudaSuccess) rc = cuda_error(err, "probe");
     }
   }
   cudaFreeAsync(base, s);
   cudaStreamSynchronize(s);
+  return rc;
+}
+
+int bbk_probe_bounded_wait(int ctas, unsigned long long timeout_ns, void* stream) {
+  if (ctas <= 0 || ctas > 255 || timeout_ns == 0)
+    return set_error(BBK_ERR_INVALID_ARGUMENT, "bad probe arguments");
+  int rc = check_device();
+  if (rc) return rc;
+  int h_status = BBK_OK;
+  rc = run_probe(ctas, ctas + 1, 1, timeout_ns, nullptr, &h_status, static_cast<cudaStream_t>(stream));
   if (rc) return rc;
   if (h_status != BBK_OK) return set_error(h_status, "bounded wait expired as designed");
   return set_error(BBK_ERR_LOGIC, "bounded-wait probe finished without timing out");
+}
+
+int bbk_probe_exchange_ns(int ctas, int iters, double* ns_per_exchange, void* stream) {
+  if (ctas <= 0 || ctas > 255 || iters <= 0 || !ns_per_exchange)
+    return set_error(BBK_ERR_INVALID_ARGUMENT, "bad probe arguments");
+  int rc = check_device();
+  if (rc) return rc;
+  int h_status = BBK_OK;
+  unsigned long long ns = 0;
+  rc = run_probe(ctas, ctas, iters, wait_timeout_ns(), &ns, &h_status, static_cast<cudaStream_t>(stream));
+  if (rc) return rc;
+  if (h_status != BBK_OK) return set_error(h_status, "exchange probe aborted");
+  *ns_per_exchange = static_cast<double>(ns) / iters;
+  return BBK_OK;
 }
 
 }  // extern "C"

@@ -30,6 +30,7 @@
 // only after the next exchange.
 #include <climits>
 #include <cstdio>
+#include <cstdlib>
 
 #include "bbk_internal.cuh"
 
@@ -38,6 +39,8 @@ namespace {
 
 constexpr int kThreads = 128;
 constexpr int kWarps = kThreads / 32;
+constexpr int kCols = 4;  // columns per thread: S <= kCols * kThreads
+constexpr int kMaxPollPerLane = 8;  // exchange records polled per lane (grid <= 256)
 
 struct PanelArgs {
   int n;
@@ -52,6 +55,7 @@ struct PanelArgs {
   int ldu;
   double* uout;
   double* wc;
+  double* wstage;    // 2 x coef_cap: W columns p and p+1 for an interchange
   int* perm;
   int* ptype;
   int* panel_end;
@@ -61,6 +65,12 @@ struct PanelArgs {
   int slot_stride;   // records per parity in `slots` (>= nslots)
   unsigned tag_base;
   unsigned long long timeout_ns;
+  int coef_cap;      // doubles reserved for the coefficient column
+  int w_smem;        // keep this CTA's workspace slice in shared memory
+  int smem_cols;     // slice width the shared-memory allocation holds
+  unsigned long long* stats;  // optional per-phase nanoseconds (CTA 0)
+  unsigned long long* pub_ts; // with stats: each CTA's publish timestamp
+  unsigned poll_ns;           // pause between polls of the exchange records
 };
 
 struct ExchangeOut {
@@ -73,27 +83,6 @@ struct ExchangeOut {
 __device__ __forceinline__ void fail(DeviceState* st, int code) {
   atomicCAS(&st->status, 0, code);
   atomicExch(&st->abort, 1);
-}
-
-// Spin until all `nw` words at p carry `tag`; false on abort or timeout.
-__device__ bool spin_tagged(const unsigned long long* p, int nw, unsigned tag,
-                            unsigned long long* out, DeviceState* st,
-                            unsigned long long t0, unsigned long long limit) {
-  for (unsigned iter = 1;; ++iter) {
-    bool ok = true;
-    for (int k = 0; k < nw; ++k) {
-      out[k] = ld_relaxed_u64(p + k);
-      ok &= static_cast<unsigned>(out[k] >> 32) == tag;
-    }
-    if (ok) return true;
-    if ((iter & 31u) == 0) {
-      if (ld_relaxed_s32(&st->abort)) return false;
-      if (globaltimer_ns() - t0 > limit) {
-        fail(st, BBK_ERR_TIMEOUT);
-        return false;
-      }
-    }
-  }
 }
 
 __device__ __forceinline__ double join_hi_lo(unsigned long long hi, unsigned long long lo) {
@@ -129,53 +118,126 @@ __device__ void exchange(const PanelArgs& P, unsigned tag, double my_val, int my
     s_red_v[warp] = my_val;
     s_red_i[warp] = my_idx;
   }
-  __syncthreads();  // also orders this CTA's global writes before the fence
-  unsigned long long* rec =
-      P.slots + (static_cast<size_t>(tag & 1u) * P.slot_stride + blockIdx.x) * kSlotWords;
-  if (t == 0) {
+  __syncthreads();  // also orders this CTA's global writes before the fences
+  // Structure-of-arrays records: word w of CTA c lives at
+  // slots[((tag & 1) * kSlotWords + w) * slot_stride + c], so one warp load
+  // polls word w of 32 consecutive CTAs in two cache lines.
+  unsigned long long* par_base =
+      P.slots + static_cast<size_t>(tag & 1u) * kSlotWords * P.slot_stride;
+  if (warp == 0) {
     double v = s_red_v[0];
     int i = s_red_i[0];
     for (int k = 1; k < kWarps; ++k) argmax_join(v, i, s_red_v[k], s_red_i[k]);
-    const unsigned long long bits = static_cast<unsigned long long>(__double_as_longlong(v));
-    fence_acq_rel_gpu();  // release everything this CTA wrote so far
-    st_relaxed_u64(rec + 0, tag_word(tag, static_cast<unsigned>(i)));
-    st_relaxed_u64(rec + 1, tag_word(tag, static_cast<unsigned>(bits >> 32)));
-    st_relaxed_u64(rec + 2, tag_word(tag, static_cast<unsigned>(bits)));
-    for (int k = 0; k < npub; ++k) {
-      const unsigned long long pb =
-          static_cast<unsigned long long>(__double_as_longlong(pub_in[k]));
-      st_relaxed_u64(rec + 3 + 2 * k, tag_word(tag, static_cast<unsigned>(pb >> 32)));
-      st_relaxed_u64(rec + 4 + 2 * k, tag_word(tag, static_cast<unsigned>(pb)));
+    // one record word per lane: (tag | idx), (tag | hi v), (tag | lo v), pubs
+    if (lane < 3 + 2 * npub) {
+      unsigned word;
+      if (lane == 0) {
+        word = static_cast<unsigned>(i);
+      } else {
+        const double x = lane < 3 ? v : pub_in[(lane - 3) >> 1];
+        const unsigned long long bits = static_cast<unsigned long long>(__double_as_longlong(x));
+        const bool high = lane < 3 ? lane == 1 : ((lane - 3) & 1) == 0;
+        word = high ? static_cast<unsigned>(bits >> 32) : static_cast<unsigned>(bits);
+      }
+      if (P.pub_ts && lane == 0) P.pub_ts[blockIdx.x] = globaltimer_ns();
+      fence_acq_rel_gpu();  // release everything this CTA wrote so far
+      st_relaxed_u64(par_base + static_cast<size_t>(lane) * P.slot_stride + blockIdx.x,
+                     tag_word(tag, word));
     }
   }
   if (warp == 0) {
-    const unsigned long long* base =
-        P.slots + static_cast<size_t>(tag & 1u) * P.slot_stride * kSlotWords;
+    // Every lane polls all of its records (CTAs lane, lane+32, ...) and its
+    // published word pair at once, so the exchange completes one L2 round trip
+    // after the last record lands.
+    const size_t st = P.slot_stride;
+    const unsigned long long* src[kMaxPollPerLane];
+    unsigned long long wv[kMaxPollPerLane][3];
+    int nmine = 0;
+    for (int sidx = lane; sidx < P.nslots && nmine < kMaxPollPerLane; sidx += 32)
+      src[nmine++] = par_base + sidx;
+    const bool has_pub = lane < npub;
+    const unsigned long long* psrc =
+        has_pub ? par_base + static_cast<size_t>(3 + 2 * lane) * st + pub_owner[lane] : par_base;
+    unsigned pending = (1u << nmine) - 1u;
+    bool pub_pending = has_pub;
+    unsigned long long pw0 = 0, pw1 = 0;
     const unsigned long long t0 = globaltimer_ns();
     bool ok = true;
-    double v = 0.0;
-    int i = INT_MAX;
-    unsigned long long wbuf[3];
-    for (int s = lane; s < P.nslots && ok; s += 32) {
-      ok = spin_tagged(base + static_cast<size_t>(s) * kSlotWords, 3, tag, wbuf, P.st, t0,
-                       P.timeout_ns);
-      if (ok) argmax_join(v, i, join_hi_lo(wbuf[1], wbuf[2]), static_cast<int>(wbuf[0] & 0xffffffffu));
-    }
-    double pubv = 0.0;
-    if (ok && lane < npub) {
-      unsigned long long pw[2];
-      ok = spin_tagged(base + static_cast<size_t>(pub_owner[lane]) * kSlotWords + 3 + 2 * lane,
-                       2, tag, pw, P.st, t0, P.timeout_ns);
-      if (ok) pubv = join_hi_lo(pw[0], pw[1]);
+    for (unsigned iter = 1; pending || pub_pending; ++iter) {
+#pragma unroll
+      for (int k = 0; k < kMaxPollPerLane; ++k) {
+        if (pending & (1u << k)) {
+          wv[k][0] = ld_relaxed_u64(src[k]);
+          wv[k][1] = ld_relaxed_u64(src[k] + st);
+          wv[k][2] = ld_relaxed_u64(src[k] + 2 * st);
+        }
+      }
+      if (pub_pending) {
+        pw0 = ld_relaxed_u64(psrc);
+        pw1 = ld_relaxed_u64(psrc + st);
+      }
+#pragma unroll
+      for (int k = 0; k < kMaxPollPerLane; ++k) {
+        if ((pending & (1u << k)) && static_cast<unsigned>(wv[k][0] >> 32) == tag &&
+            static_cast<unsigned>(wv[k][1] >> 32) == tag && static_cast<unsigned>(wv[k][2] >> 32) == tag)
+          pending &= ~(1u << k);
+      }
+      if (pub_pending && static_cast<unsigned>(pw0 >> 32) == tag && static_cast<unsigned>(pw1 >> 32) == tag)
+        pub_pending = false;
+      if (P.poll_ns && (pending || pub_pending)) __nanosleep(P.poll_ns);
+      if ((iter & 31u) == 0 && (pending || pub_pending)) {
+        if (ld_relaxed_s32(&P.st->abort)) {
+          ok = false;
+          break;
+        }
+        if (globaltimer_ns() - t0 > P.timeout_ns) {
+          fail(P.st, BBK_ERR_TIMEOUT);
+          ok = false;
+          break;
+        }
+      }
     }
     fence_acq_rel_gpu();  // acquire what the other CTAs released
+    double v = 0.0;
+    int i = INT_MAX;
+    if (ok) {
+      for (int k = 0; k < nmine; ++k)
+        argmax_join(v, i, join_hi_lo(wv[k][1], wv[k][2]), static_cast<int>(wv[k][0] & 0xffffffffu));
+    }
     for (int off = 16; off > 0; off >>= 1) {
       const double v2 = __shfl_down_sync(0xffffffffu, v, off);
       const int i2 = __shfl_down_sync(0xffffffffu, i, off);
       argmax_join(v, i, v2, i2);
     }
     const int all_ok = __all_sync(0xffffffffu, ok);
-    if (lane < npub) out->pub[lane] = pubv;
+    if (P.pub_ts && blockIdx.x == 0 && all_ok) {
+      // diagnostics: (last publish - own publish) and (done - last publish)
+      const unsigned long long done = globaltimer_ns();
+      unsigned long long last = 0;
+      int who = 0;
+      for (int sidx = lane; sidx < P.nslots; sidx += 32) {
+        const unsigned long long v = __ldcg(P.pub_ts + sidx);
+        if (v > last) {
+          last = v;
+          who = sidx;
+        }
+      }
+      for (int off = 16; off > 0; off >>= 1) {
+        const unsigned long long l2 = __shfl_down_sync(0xffffffffu, last, off);
+        const int w2 = __shfl_down_sync(0xffffffffu, who, off);
+        if (l2 > last) {
+          last = l2;
+          who = w2;
+        }
+      }
+      if (lane == 0) {
+        const unsigned long long mine = __ldcg(P.pub_ts);
+        atomicAdd(P.stats + 7, last > mine ? last - mine : 0ull);
+        atomicAdd(P.stats + 8, done > last ? done - last : 0ull);
+        atomicAdd(P.stats + 16 + 1024 + who, 1ull);
+      }
+    }
+    if (has_pub) out->pub[lane] = join_hi_lo(pw0, pw1);
     if (lane == 0) {
       out->val = v;
       out->idx = i;
@@ -195,6 +257,7 @@ __device__ __forceinline__ double div_or_zero(double x, double den) {
 }
 
 __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
+  extern __shared__ double dsm[];
   __shared__ double s_red_v[kWarps];
   __shared__ int s_red_i[kWarps];
   __shared__ double s_pub[kMaxPub];
@@ -212,36 +275,74 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
   const long long lda = P.lda, ldw = P.ldw;
   const int ldu = P.ldu;
   auto owner = [&](int j) -> int { return (j - kstart) / S; };
+  // shared memory: coefficient column, then (when it fits) this CTA's slice
+  // of the panel's workspace rows, wsm[q*S + (j - lo)] = W[q, j].
+  // Stores other CTAs do not need right away stay out of global memory: the
+  // slice of W (flushed at the end of the panel) and the candidate column.
+  double* coef = dsm;
+  double* wcs = dsm + P.coef_cap;  // candidate values of this CTA's columns
+  double* wsm = (P.w_smem && S <= P.smem_cols) ? wcs + P.smem_cols : nullptr;
+  auto wget = [&](int q, int j) -> double {
+    return wsm ? wsm[q * S + (j - lo)] : ldcg(P.w + q * ldw + j);
+  };
+  auto wput = [&](int q, int j, double v) {
+    if (wsm)
+      wsm[q * S + (j - lo)] = v;
+    else
+      P.w[q * ldw + j] = v;
+  };
+  const bool timing = P.stats != nullptr && t == 0;
+  unsigned long long tm[6] = {0, 0, 0, 0, 0, 0};
+  unsigned long long tmark = timing ? globaltimer_ns() : 0;
+  auto lap = [&](int k) {
+    if (timing) {
+      const unsigned long long now = globaltimer_ns();
+      tm[k] += now - tmark;
+      tmark = now;
+    }
+  };
 
   unsigned tag = P.tag_base;
   int p = kstart;
   // coefficients U[q, p] of the current row: rows q < n_old from Ucm column
-  // coef_src, then n_extra (<= 2) values computed by every CTA.
-  int coef_src = p, n_old = 0, n_extra = 0;
+  // coef_src, then lp - n_old (<= 2) values computed by every CTA.
+  int coef_src = p, n_old = 0;
   double extra0 = 0.0, extra1 = 0.0;
   int fix_col = -1;          // A[p][fix_col] must be read from fix_src
   long long fix_src = 0;
-  int shifted = 0;
+  int ncand = 0;
 
   while (p < P.nominal_end) {
     const int lp = p - kstart;
+    const int jbeg = max(lo, p);
     // ---- row update: W[p, j] = A[p, j] - sum_q U[q, p] W[q, j]
     // (CopyCurrentRowToWorkspace + UpdateCurrentRowInWorkspace, :122-162)
-    double best = 0.0;
-    int best_j = INT_MAX;
-    if (t < kMaxPub) s_pub[t] = 0.0;
-    __syncthreads();
+    double av[kCols];
+#pragma unroll
+    for (int k = 0; k < kCols; ++k) {
+      const int j = jbeg + t + k * kThreads;
+      av[k] = j < hi ? ((j == fix_col) ? ldcg(P.a + fix_src) : ldcg(P.a + p * lda + j)) : 0.0;
+    }
     {
       const double* ucol = P.ucm + static_cast<size_t>(coef_src) * ldu;
-      for (int j = max(lo, p) + t; j < hi; j += kThreads) {
+      for (int q = t; q < n_old; q += kThreads) coef[q] = ldcg(ucol + q);
+      if (t == 0) {
+        coef[n_old] = extra0;
+        coef[n_old + 1] = extra1;
+      }
+      if (t < kMaxPub) s_pub[t] = 0.0;
+    }
+    __syncthreads();
+    double best = 0.0;
+    int best_j = INT_MAX;
+#pragma unroll
+    for (int k = 0; k < kCols; ++k) {
+      const int j = jbeg + t + k * kThreads;
+      if (j < hi) {
         double acc = 0.0;
-        for (int q = 0; q < n_old; ++q)
-          acc = xadd(acc, xmul(ldcg(ucol + q), ldcg(P.w + q * ldw + j)));
-        if (n_extra > 0) acc = xadd(acc, xmul(extra0, ldcg(P.w + n_old * ldw + j)));
-        if (n_extra > 1) acc = xadd(acc, xmul(extra1, ldcg(P.w + (n_old + 1) * ldw + j)));
-        const double av = (j == fix_col) ? ldcg(P.a + fix_src) : ldcg(P.a + p * lda + j);
-        const double wv = xsub(av, acc);
-        P.w[lp * ldw + j] = wv;
+        for (int q = 0; q < lp; ++q) acc = xadd(acc, xmul(coef[q], wget(q, j)));
+        const double wv = xsub(av[k], acc);
+        wput(lp, j, wv);
         if (j > p) {
           const double v = fabs(wv);
           if (v > best) {  // FindCurrentRowMax, :164-182
@@ -256,6 +357,7 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
       }
     }
     fix_col = -1;
+    lap(0);
     int owners[kMaxPub];
     owners[0] = owner(p);
     owners[1] = p + 1 < n ? owner(p + 1) : 0;
@@ -268,6 +370,7 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
     const double w_p1 = s_x.pub[1];  // W[p, p+1] (current-row version)
     const double w_p2 = s_x.pub[2];  // W[p, p+2]
     __syncthreads();
+    lap(1);
 
     int kind = 1;  // 1: 1x1 at p; -1: 1x1 after p<->r; 2: 2x2 with p+1<->r
     bool cand = false;
@@ -275,29 +378,47 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
     // FactorPanel's test, :90-92
     if (!(fabs(dpp) >= xmul(kAlpha, omega) || omega == 0.0)) {
       cand = true;
+      ++ncand;
       // ---- candidate column W(i, r) = A(i, r) - sum_q U[q, r] W[q, i]
       // (CopyCandidateToWorkspace + UpdateCandidateInWorkspace, :184-352)
-      if (t < kMaxPub) s_pub[t] = 0.0;
+#pragma unroll
+      for (int k = 0; k < kCols; ++k) {
+        const int i = jbeg + t + k * kThreads;
+        av[k] = i < hi ? (i <= r ? ldcg(P.a + i * lda + r) : ldcg(P.a + r * lda + i)) : 0.0;
+      }
+      {
+        const double* ucol = P.ucm + static_cast<size_t>(r) * ldu;
+        for (int q = t; q < lp; q += kThreads) coef[q] = ldcg(ucol + q);
+        if (t < kMaxPub) s_pub[t] = 0.0;
+      }
       __syncthreads();
       double sig = 0.0;
-      const double* ucol = P.ucm + static_cast<size_t>(r) * ldu;
-      for (int i = max(lo, p) + t; i < hi; i += kThreads) {
-        double acc = 0.0;
-        for (int q = 0; q < lp; ++q)
-          acc = xadd(acc, xmul(ldcg(ucol + q), ldcg(P.w + q * ldw + i)));
-        const double av = i <= r ? ldcg(P.a + i * lda + r) : ldcg(P.a + r * lda + i);
-        const double v = xsub(av, acc);
-        P.wc[i] = v;
-        if (i != r) {
-          const double av2 = fabs(v);
-          sig = (sig < av2) ? av2 : sig;  // std::max, FindCandidateColumnMax :354-367
-        } else {
-          s_pub[0] = v;
+#pragma unroll
+      for (int k = 0; k < kCols; ++k) {
+        const int i = jbeg + t + k * kThreads;
+        if (i < hi) {
+          double acc = 0.0;
+          for (int q = 0; q < lp; ++q) acc = xadd(acc, xmul(coef[q], wget(q, i)));
+          const double v = xsub(av[k], acc);
+          wcs[i - lo] = v;
+          if (i != r) {
+            const double av2 = fabs(v);
+            sig = (sig < av2) ? av2 : sig;  // std::max, FindCandidateColumnMax :354-367
+          } else {
+            s_pub[0] = v;
+          }
+          if (i == p) s_pub[1] = v;
+          if (i == p + 1) s_pub[2] = v;
+          if (i == p + 2) s_pub[3] = v;
         }
-        if (i == p) s_pub[1] = v;
-        if (i == p + 1) s_pub[2] = v;
-        if (i == p + 2) s_pub[3] = v;
       }
+      // stage W[q, p] and W[q, p+1] (q < lp) for the owner of r: the
+      // interchange moves one of these columns into column r
+      if (p >= lo && p < hi)
+        for (int q = t; q < lp; q += kThreads) P.wstage[q] = wget(q, p);
+      if (p + 1 >= lo && p + 1 < hi)
+        for (int q = t; q < lp; q += kThreads) P.wstage[P.coef_cap + q] = wget(q, p + 1);
+      lap(2);
       owners[0] = owner(r);
       owners[1] = owner(p);
       owners[2] = p + 1 < n ? owner(p + 1) : 0;
@@ -310,6 +431,7 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
       wc_p1 = s_x.pub[2];
       wc_p2 = s_x.pub[3];
       __syncthreads();
+      lap(3);
       // SelectPivot, :369-390
       if (xsub(xmul(fabs(dpp), sigma), xmul(xmul(kAlpha, omega), omega)) >= 0.0) {
         kind = 1;
@@ -320,10 +442,7 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
       }
       // :104-108: a 2x2 pivot starting at the panel's last column moves that
       // column into the next panel (ShiftBoundaryColumnToNextBlock).
-      if (kind == 2 && p == P.nominal_end - 1 && P.can_shift) {
-        shifted = 1;
-        break;
-      }
+      if (kind == 2 && p == P.nominal_end - 1 && P.can_shift) break;
     }
 
     if (kind == 1) {
@@ -335,9 +454,9 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
         double wv;
         if (cand && j == r) {
           wv = wc_p;
-          P.w[lp * ldw + j] = wv;
+          wput(lp, j, wv);
         } else {
-          wv = P.w[lp * ldw + j];
+          wv = wget(lp, j);
         }
         P.ucm[static_cast<size_t>(j) * ldu + lp] = div_or_zero(wv, den);
       }
@@ -352,7 +471,6 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
       // next row's coefficients: U[q, p+1] for q < p, then U[p, p+1]
       coef_src = p + 1;
       n_old = lp;
-      n_extra = 1;
       extra0 = div_or_zero((cand && r == p + 1) ? wc_p : w_p1, den);
       p += 1;
     } else if (kind == -1) {
@@ -361,11 +479,11 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
       const double den = safe_denominator(d);
       for (int j = max(lo, p) + t; j < hi; j += kThreads) {
         if (j == p) {
-          P.w[lp * ldw + j] = d;
+          wput(lp, j, d);
           continue;
         }
-        const double wv = (j == r) ? wc_p : P.wc[j];
-        P.w[lp * ldw + j] = wv;
+        const double wv = (j == r) ? wc_p : wcs[j - lo];
+        wput(lp, j, wv);
         P.ucm[static_cast<size_t>(j) * ldu + lp] = div_or_zero(wv, den);
         // old row p moves to row r (j > r) / column r (j < r); row p itself
         // stays frozen so other CTAs may still read it.
@@ -383,7 +501,7 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
           const double ur = ldcg(P.ucm + static_cast<size_t>(r) * ldu + q);
           P.uout[static_cast<size_t>(lp) * ldu + q] = ur;  // final column p
           P.ucm[static_cast<size_t>(r) * ldu + q] = ldcg(P.ucm + static_cast<size_t>(p) * ldu + q);
-          P.w[q * ldw + r] = ldcg(P.w + q * ldw + p);
+          wput(q, r, ldcg(P.wstage + q));
         }
       }
       // previously factored rows: columns p and r exchange (:472-491)
@@ -403,7 +521,6 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
       }
       coef_src = (r == p + 1) ? p : p + 1;
       n_old = lp;
-      n_extra = 1;
       extra0 = div_or_zero((r == p + 1) ? wc_p : wc_p1, den);
       if (p + 1 < r) {
         fix_col = r;
@@ -422,12 +539,12 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
         double x;
         if (j == r) {
           x = w_p1;  // W(p, s) and W(p, r) exchange
-          P.w[lp * ldw + j] = x;
+          wput(lp, j, x);
         } else {
-          x = P.w[lp * ldw + j];
+          x = wget(lp, j);
         }
-        const double y = (j == r) ? wc_p1 : P.wc[j];
-        P.w[ls * ldw + j] = y;
+        const double y = (j == r) ? wc_p1 : wcs[j - lo];
+        wput(ls, j, y);
         P.ucm[static_cast<size_t>(j) * ldu + lp] = xadd(xmul(i11, x), xmul(i21, y));
         P.ucm[static_cast<size_t>(j) * ldu + ls] = xadd(xmul(i21, x), xmul(i22, y));
         if (r != s) {
@@ -451,7 +568,7 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
           P.uout[static_cast<size_t>(ls) * ldu + q] = ur;  // final column s
           if (r != s) {
             P.ucm[static_cast<size_t>(r) * ldu + q] = ldcg(P.ucm + static_cast<size_t>(s) * ldu + q);
-            P.w[q * ldw + r] = ldcg(P.w + q * ldw + s);
+            wput(q, r, ldcg(P.wstage + P.coef_cap + q));
           }
         }
       }
@@ -479,7 +596,6 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
       const double y = (r == p + 2) ? wc_p1 : wc_p2;
       coef_src = (r == p + 2) ? s : p + 2;
       n_old = lp;
-      n_extra = 2;
       extra0 = xadd(xmul(i11, x), xmul(i21, y));
       extra1 = xadd(xmul(i21, x), xmul(i22, y));
       if (p + 2 < r) {
@@ -489,14 +605,27 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
       p += 2;
     }
     __syncthreads();
+    lap(4);
   }
 
+  if (P.stats && t == 0)
+    for (int k = 0; k < 5; ++k) atomicAdd(P.stats + 16 + 2048 + c * 5 + k, tm[k]);
+  // the trailing update reads W from global memory
+  if (wsm) {
+    const int kb = p - kstart;
+    for (int q = 0; q < kb; ++q)
+      for (int j = lo + t; j < hi; j += kThreads) P.w[q * ldw + j] = wsm[q * S + (j - lo)];
+  }
   if (c == 0 && t == 0) {
     // panel range [kstart, p); the next panel starts at p.
     P.st->kstart[(P.panel + 1) & 1] = p;
     if (P.panel_end) P.panel_end[P.panel] = p;
+    if (P.stats) {
+      for (int k = 0; k < 5; ++k) atomicAdd(P.stats + k, tm[k]);
+      atomicAdd(P.stats + 5, static_cast<unsigned long long>(p - kstart));
+      atomicAdd(P.stats + 6, static_cast<unsigned long long>(ncand));
+    }
   }
-  (void)shifted;
 }
 
 // Writes the panel's compact factor rows [k0, e) into A:
@@ -558,8 +687,11 @@ __global__ void status_copy_kernel(const DeviceState* st, int* out) {
   if (threadIdx.x == 0 && blockIdx.x == 0) *out = st->status;
 }
 
-// Bounded-wait probe: one exchange that also waits for a record nobody
-// writes (nslots = gridDim.x + 1), so it must end by timeout.
+// Exchange probe.  With nslots == gridDim.x + 1 the single exchange also
+// waits for a record nobody writes, so it must end by timeout (the
+// bounded-wait test).  With nslots == gridDim.x it runs `iters` exchanges
+// back to back and CTA 0 stores the elapsed nanoseconds in stats[0] (the
+// exchange-latency measurement).
 __global__ void __launch_bounds__(kThreads) probe_kernel(PanelArgs P) {
   __shared__ double s_red_v[kWarps];
   __shared__ int s_red_i[kWarps];
@@ -568,7 +700,13 @@ __global__ void __launch_bounds__(kThreads) probe_kernel(PanelArgs P) {
   if (threadIdx.x < kMaxPub) s_pub[threadIdx.x] = 0.0;
   int owners[kMaxPub] = {0, 0, 0, 0, 0, 0};
   __syncthreads();
-  exchange(P, P.tag_base, 0.0, 0, s_pub, owners, 0, s_red_v, s_red_i, &s_x);
+  const unsigned long long t0 = globaltimer_ns();
+  for (int it = 0; it < P.n; ++it) {
+    exchange(P, P.tag_base + it, static_cast<double>(blockIdx.x), blockIdx.x, s_pub, owners, 3,
+             s_red_v, s_red_i, &s_x);
+    if (!s_x.ok) return;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0 && P.stats) P.stats[0] = globaltimer_ns() - t0;
 }
 
 }  // namespace
@@ -582,13 +720,24 @@ static int cooperative_launch(const void* fn, int grid, PanelArgs* args, cudaStr
 }
 
 int panel_grid_size(int n) {
-  // enough CTAs that each owns <= 128 columns, at most one per SM
+  // enough CTAs that each owns <= 64 columns where possible, at most one per
+  // SM, and never more than kCols columns per thread.  BBK_PANEL_COLS
+  // overrides the target columns per CTA (tuning).
   const int sms = device_sm_count();
-  int g = (n + 63) / 64;
+  static const int cols = [] {
+    const char* e = getenv("BBK_PANEL_COLS");
+    const int v = e ? atoi(e) : 0;
+    return v > 0 ? v : 64;
+  }();
+  int g = (n + cols - 1) / cols;
   if (g > sms) g = sms;
+  const int need = (n + kCols * kThreads - 1) / (kCols * kThreads);
+  if (g < need) g = need;
   if (g < 1) g = 1;
   return g;
 }
+
+int panel_max_n() { return device_sm_count() * kCols * kThreads; }
 
 int launch_init(int n, int* perm, int* pivot_types, DeviceState* st, unsigned long long* slots,
                 size_t slot_words, cudaStream_t s) {
@@ -613,6 +762,7 @@ int launch_panel(const FactorPlan& plan, int panel, cudaStream_t s) {
   P.ldu = plan.ldu;
   P.uout = plan.uout;
   P.wc = plan.wc;
+  P.wstage = plan.wc + align_up(static_cast<size_t>(plan.n), 64);
   P.perm = plan.perm;
   P.ptype = plan.pivot_types;
   P.panel_end = plan.panel_end;
@@ -623,7 +773,32 @@ int launch_panel(const FactorPlan& plan, int panel, cudaStream_t s) {
   // tags: distinct for every exchange of the call (slots are zeroed per call)
   P.tag_base = 1u + static_cast<unsigned>(panel) * (2u * static_cast<unsigned>(plan.b) + 8u);
   P.timeout_ns = plan.timeout_ns;
-  return cooperative_launch(reinterpret_cast<const void*>(panel_kernel), plan.grid, &P, s);
+  P.stats = plan.stats;
+  P.pub_ts = plan.stats ? plan.stats + 16 : nullptr;
+  static const unsigned poll_ns = [] {
+    const char* e = getenv("BBK_POLL_NS");
+    return e ? static_cast<unsigned>(atoi(e)) : 0u;
+  }();
+  P.poll_ns = poll_ns;
+  if (plan.grid > 32 * kMaxPollPerLane)
+    return set_error(BBK_ERR_INVALID_ARGUMENT, "panel grid %d exceeds %d", plan.grid, 32 * kMaxPollPerLane);
+  // shared memory: coefficient column + (if it fits) the CTA's W slice
+  const int smax = (plan.n + plan.grid - 1) / plan.grid;
+  P.coef_cap = static_cast<int>(align_up(static_cast<size_t>(plan.b) + 4, 2));
+  size_t bytes = (static_cast<size_t>(P.coef_cap) + smax) * sizeof(double);
+  const size_t wbytes = static_cast<size_t>(plan.b + 2) * smax * sizeof(double);
+  const size_t limit = 220 * 1024;
+  P.w_smem = bytes + wbytes <= limit;
+  P.smem_cols = smax;
+  if (P.w_smem) bytes += wbytes;
+  BBK_CUDA_TRY(cudaFuncSetAttribute(panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(bytes)));
+  void* kargs[] = {&P};
+  cudaError_t err = cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(panel_kernel),
+                                                dim3(plan.grid), dim3(kThreads), kargs, bytes, s);
+  if (err != cudaSuccess) return cuda_error(err, "cudaLaunchCooperativeKernel(panel)");
+  count_launch();
+  return BBK_OK;
 }
 
 int launch_finalize(const FactorPlan& plan, int panel, cudaStream_t s) {
@@ -642,15 +817,18 @@ int launch_status_copy(const DeviceState* st, int* status_out, cudaStream_t s) {
   return BBK_OK;
 }
 
-int launch_probe_wait(int ctas, unsigned long long timeout_ns, DeviceState* st,
-                      unsigned long long* slots, cudaStream_t s) {
+int launch_probe_wait(int ctas, int nslots, int iters, unsigned long long timeout_ns,
+                      DeviceState* st, unsigned long long* slots, unsigned long long* stats,
+                      cudaStream_t s) {
   PanelArgs P{};
   P.slots = slots;
   P.st = st;
-  P.nslots = ctas + 1;  // one participant that never arrives
+  P.nslots = nslots;
   P.slot_stride = ctas + 1;
   P.tag_base = 7u;
   P.timeout_ns = timeout_ns;
+  P.n = iters;
+  P.stats = stats;
   return cooperative_launch(reinterpret_cast<const void*>(probe_kernel), ctas, &P, s);
 }
 

@@ -20,13 +20,10 @@ namespace {
 
 constexpr int kSB = 64;           // solve block
 constexpr int kSolveThreads = 256;
-constexpr int kRowsPerCta = 256;  // rows updated per CTA
+constexpr int kRowsPerCta = 256;  // forward: rows updated per CTA (one per thread)
+constexpr int kRowsBack = 64;     // backward: rows updated per CTA (warp per row)
 constexpr int kMaxRhsChunk = 8;   // right-hand sides per pass
-
-__device__ __forceinline__ bool coupled(const int* pt, int k, int i) {
-  // L(i,k) is structurally zero inside a 2x2 pivot block
-  return i == k + 1 && pt[k] == 2;
-}
+constexpr int kKChunk = 16;       // coefficient loads kept in flight per thread
 
 __global__ void gather_kernel(int n, int nrhs, const double* b, long long ldb, const int* perm,
                               double* y) {
@@ -89,9 +86,18 @@ __global__ void __launch_bounds__(kSolveThreads) sweep_kernel(int n, int nrhs, c
   __shared__ int pts[kSB];
   const int bs = k1 - k0;
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  for (int idx = t; idx < kSB * kSB; idx += kSolveThreads) {
-    const int r = idx / kSB, c = idx % kSB;
-    fs[r][c] = (r < c && c < bs) ? f[static_cast<long long>(k0 + r) * ldf + k0 + c] : 0.0;
+  {
+    double v[kSB * kSB / kSolveThreads];
+#pragma unroll
+    for (int it = 0; it < kSB * kSB / kSolveThreads; ++it) {
+      const int idx = t + it * kSolveThreads, r = idx / kSB, c = idx % kSB;
+      v[it] = (r < c && c < bs) ? f[static_cast<long long>(k0 + r) * ldf + k0 + c] : 0.0;
+    }
+#pragma unroll
+    for (int it = 0; it < kSB * kSB / kSolveThreads; ++it) {
+      const int idx = t + it * kSolveThreads;
+      fs[idx / kSB][idx % kSB] = v[it];
+    }
   }
   for (int r = t; r < kSB; r += kSolveThreads) pts[r] = r < bs ? pt[k0 + r] : 1;
   // the 2x2 coupling can straddle the block edge: pivot k0-1 with k0
@@ -134,42 +140,54 @@ __global__ void __launch_bounds__(kSolveThreads) sweep_kernel(int n, int nrhs, c
     }
     // ---- contribution of the block to the other rows
     if (kForward) {
-      const int rows = n - k1;
-      for (int i = k1 + blockIdx.x * kRowsPerCta + t; i < n && i < k1 + (blockIdx.x + 1) * kRowsPerCta;
-           i += kSolveThreads) {
+      const int i = k1 + blockIdx.x * kRowsPerCta + t;
+      if (i < n) {
         double acc[kMaxRhsChunk];
 #pragma unroll
         for (int cc = 0; cc < kMaxRhsChunk; ++cc) acc[cc] = 0.0;
-        for (int k = 0; k < bs; ++k) {
-          if (i == k0 + k + 1 && pts[k] == 2) continue;
-          const double l = f[static_cast<long long>(k0 + k) * ldf + i];
+        for (int kc = 0; kc < bs; kc += kKChunk) {
+          double l[kKChunk];
 #pragma unroll
-          for (int cc = 0; cc < kMaxRhsChunk; ++cc)
-            if (cc < nc) acc[cc] += l * ys[cc][k];
+          for (int kk = 0; kk < kKChunk; ++kk) {
+            const int k = kc + kk;
+            const bool ok = k < bs && !(i == k0 + k + 1 && pts[k] == 2);
+            l[kk] = ok ? f[static_cast<long long>(k0 + k) * ldf + i] : 0.0;
+          }
+#pragma unroll
+          for (int kk = 0; kk < kKChunk; ++kk)
+#pragma unroll
+            for (int cc = 0; cc < kMaxRhsChunk; ++cc)
+              if (cc < nc && kc + kk < bs) acc[cc] += l[kk] * ys[cc][kc + kk];
         }
         for (int cc = 0; cc < nc; ++cc) y[static_cast<long long>(c0 + cc) * n + i] -= acc[cc];
       }
-      (void)rows;
     } else {
-      // rows i < k0, F(i, k0..k1) contiguous: one warp per row
-      const int rows_lo = blockIdx.x * kRowsPerCta;
-      const int rows_hi = min(k0, rows_lo + kRowsPerCta);
-      for (int i = rows_lo + warp; i < rows_hi; i += kSolveThreads / 32) {
-        double acc[kMaxRhsChunk];
+      // rows i < k0, F(i, k0..k1) contiguous: one warp per row, four rows per
+      // pass so every lane keeps eight loads in flight
+      const int rows_lo = blockIdx.x * kRowsBack;
+      const int rows_hi = min(k0, rows_lo + kRowsBack);
+      constexpr int kR = 4;
+      for (int i0 = rows_lo + warp * kR; i0 < rows_hi; i0 += kR * (kSolveThreads / 32)) {
+        double l[kR][2];
 #pragma unroll
-        for (int cc = 0; cc < kMaxRhsChunk; ++cc) acc[cc] = 0.0;
-        for (int k = lane; k < bs; k += 32) {
-          if (k == 0 && i == k0 - 1 && pt_before == 2) continue;
-          const double l = f[static_cast<long long>(i) * ldf + k0 + k];
+        for (int rr = 0; rr < kR; ++rr) {
+          const int i = i0 + rr;
 #pragma unroll
-          for (int cc = 0; cc < kMaxRhsChunk; ++cc)
-            if (cc < nc) acc[cc] += l * ys[cc][k];
+          for (int h = 0; h < 2; ++h) {
+            const int k = lane + 32 * h;
+            const bool ok = i < rows_hi && k < bs && !(k == 0 && i == k0 - 1 && pt_before == 2);
+            l[rr][h] = ok ? f[static_cast<long long>(i) * ldf + k0 + k] : 0.0;
+          }
         }
+        for (int cc = 0; cc < nc; ++cc) {
+          const double y0 = lane < bs ? ys[cc][lane] : 0.0;
+          const double y1 = lane + 32 < bs ? ys[cc][lane + 32] : 0.0;
 #pragma unroll
-        for (int cc = 0; cc < kMaxRhsChunk; ++cc) {
-          double v = acc[cc];
-          for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-          if (lane == 0 && cc < nc) y[static_cast<long long>(c0 + cc) * n + i] -= v;
+          for (int rr = 0; rr < kR; ++rr) {
+            double v = l[rr][0] * y0 + l[rr][1] * y1;
+            for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+            if (lane == 0 && i0 + rr < rows_hi) y[static_cast<long long>(c0 + cc) * n + i0 + rr] -= v;
+          }
         }
       }
     }
@@ -255,7 +273,7 @@ int solve_enqueue(int n, const double* f, long long ldf, const int* perm, const 
   const int nblk = (n + kSB - 1) / kSB;
   for (int bi = nblk - 1; bi >= 0; --bi) {
     const int k0 = bi * kSB, k1 = std::min(n, k0 + kSB);
-    const int grid = std::max(1, (k0 + kRowsPerCta - 1) / kRowsPerCta);
+    const int grid = std::max(1, (k0 + kRowsBack - 1) / kRowsBack);
     sweep_kernel<false><<<grid, kSolveThreads, 0, s>>>(n, nrhs, f, ldf, pivot_types, z, y, k0, k1);
     BBK_CUDA_TRY(cudaGetLastError());
     count_launch();

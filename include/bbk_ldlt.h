@@ -68,10 +68,34 @@ unsigned long long bbk_kernel_launch_count(void);
  * BBK_ERR_TIMEOUT instead of hanging.  Default 5 s. */
 int bbk_set_wait_timeout_ns(unsigned long long timeout_ns);
 /* Test hook for the bounded-wait machinery: launches one cooperative grid of
- * `ctas` blocks whose exchange also waits for one participant that does not
- * exist, so the wait must run out.  Returns BBK_ERR_TIMEOUT when the bound
+ * `ctas` (1..255) blocks whose exchange also waits for one participant that
+ * does not exist, so the wait must run out.  Returns BBK_ERR_TIMEOUT when the bound
  * works (and leaves the context usable), BBK_OK never. */
 int bbk_probe_bounded_wait(int ctas, unsigned long long timeout_ns, void* stream);
+/* Diagnostics: runs `iters` back-to-back grid exchanges (the panel kernel's
+ * barrier + all-gather) on `ctas` (1..255) co-resident blocks and reports the
+ * mean device nanoseconds per exchange. */
+int bbk_probe_exchange_ns(int ctas, int iters, double* ns_per_exchange, void* stream);
+
+/* Per-kernel-class device timing for benchmarks: between begin and end,
+ * every launch of this library is bracketed by CUDA events on its own
+ * stream.  end() waits for the events and writes the summed milliseconds
+ * per class into ms[0..4] = {init, panel, finalize, trailing update, solve}
+ * and the launch counts into counts[0..4] (either may be NULL). */
+int bbk_profile_begin(void);
+int bbk_profile_end(double* ms, long long* counts);
+/* Panel-kernel phase timing (diagnostics): enable != 0 zeroes and arms the
+ * counters; enable == 0 disarms them and copies 10 counters to out: summed
+ * nanoseconds of CTA 0 in {row update, first exchange, candidate column,
+ * second exchange, interchange + scaling}, pivots, candidate evaluations,
+ * (unused), and over all exchanges the summed nanoseconds between CTA 0's
+ * publish and the last CTA's publish, and between the last publish and
+ * CTA 0 seeing every record. */
+int bbk_panel_stats(int enable, unsigned long long* out);
+/* The raw diagnostic counter array behind bbk_panel_stats (first `words`
+ * words): [0..15] the counters above, then per panel-CTA how often it
+ * published last in an exchange, then per CTA its own 5 phase totals. */
+int bbk_panel_stats_raw(unsigned long long* out, size_t words);
 
 /* ---- factorization ------------------------------------------------------
  * Replaces BlockLdltDecomposition(const BlockMatrix&, mode) + Factorize()
