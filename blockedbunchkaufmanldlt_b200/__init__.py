@@ -44,8 +44,9 @@ EXPORTS = (
     "bbk_factor_device", "bbk_factor_device_async", "bbk_factor_host",
     "bbk_solve_workspace_size", "bbk_solve_device", "bbk_solve_host", "bbk_factor_solve_host",
     "bbk_reconstruct_device", "bbk_scale_one_by_one", "bbk_scale_two_by_two",
-    "bbk_update_trailing_block", "bbk_profile_begin", "bbk_profile_end", "bbk_panel_stats", "bbk_panel_stats_raw",
+    "bbk_update_trailing_block", "bbk_profile_begin", "bbk_profile_end", "bbk_panel_stats", "bbk_panel_stats_raw", "bbk_solve_device_noalloc",
 )
+SOLVE_NOALLOC_MAX_ELEMENTS = 524288  # n * nrhs limit of bbk_solve_device_noalloc
 PROFILE_CLASSES = ("init", "panel", "finalize", "update", "solve")
 
 
@@ -110,6 +111,7 @@ def lib() -> ctypes.CDLL:
         "bbk_solve_workspace_size": ([_c_int, _c_int], _c_sz),
         "bbk_solve_device": ([_c_int, _vp, _c_ll, _vp, _vp, _c_int, _vp, _c_ll, _vp, _c_sz, _vp], _c_int),
         "bbk_solve_host": ([_c_int, _vp, _c_ll, _vp, _vp, _c_int, _vp, _c_ll], _c_int),
+        "bbk_solve_device_noalloc": ([_c_int, _vp, _c_ll, _vp, _vp, _c_int, _vp, _c_ll, _vp], _c_int),
         "bbk_factor_solve_host": ([_c_int, _c_int, _vp, _c_ll, _vp, _vp, _vp, _c_int, _vp, _c_ll,
                                    _c_int], _c_int),
         "bbk_reconstruct_device": ([_c_int, _vp, _c_ll, _vp, _vp, _vp, _c_ll, _vp], _c_int),

@@ -146,6 +146,28 @@ int bbk_solve_host(int n, const double* factors, long long ldf,
                    const int* perm, const int* pivot_types, int nrhs,
                    double* b, long long ldb);
 
+/* No counterpart in the reference (which has no solve).  The same solve as
+ * bbk_solve_device, for callers that cannot allocate device memory: a
+ * framework whose caching allocator owns the device's memory, a fixed pool
+ * set up once, or a latency-critical loop that cannot afford the device-wide
+ * synchronisation of cudaMalloc/cudaFree.  It allocates nothing: its
+ * 2 * n * nrhs doubles of scratch come from one fixed 8 MiB array inside the
+ * library that every GPU loading the library holds until the process exits,
+ * so n * nrhs may be at most BBK_SOLVE_NOALLOC_MAX_ELEMENTS (larger sizes are
+ * rejected with BBK_ERR_INVALID_ARGUMENT).  The first call on each device
+ * looks up that array's device address; make that first call before any
+ * stream capture.  All calls on a device share the array and it keeps the
+ * last call's contents (nothing in it needs clearing: every element is
+ * written before it is read), so calls whose work overlaps on the GPU --
+ * different streams, or different host threads -- race and corrupt each
+ * other.  Enqueues on `stream` and returns without waiting; device
+ * pointers. */
+#define BBK_SOLVE_NOALLOC_MAX_ELEMENTS 524288
+int bbk_solve_device_noalloc(int n, const double* factors, long long ldf,
+                             const int* perm, const int* pivot_types,
+                             int nrhs, double* b, long long ldb,
+                             void* stream);
+
 /* ---- factor + solve in one call, host buffers (the end-to-end path) ----
  * a (in: matrix, out: compact factors), b (in: right-hand sides, out:
  * solutions). */
