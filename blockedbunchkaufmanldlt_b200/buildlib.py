@@ -57,8 +57,6 @@ def build(verbose: bool = False, force: bool = False) -> str:
         cmd = [nvcc()] + ARCH + NVCC_FLAGS
         if src in NO_FMAD:
             cmd.append("--fmad=false")
-        if src.endswith(".cc"):
-            cmd += ["-x", "cu"]
         cmd += ["-c", path, "-o", obj]
         if verbose:
             print(" ".join(cmd), flush=True)

@@ -10,6 +10,11 @@ reference's outputs for an input that the tests can regenerate exactly:
 * ``ref_large.json``: larger cases (seeded uniform[-1,1] inputs from numpy's
   PCG64): perm and pivot types in full, plus a SHA-256 of the compact upper
   factor's bytes so a bitwise match can be checked without storing it.
+* ``ref_geometry.txt``: cases with several boundary shifts (the reference
+  tests' generator, so C++ can regenerate the input): the reference's block
+  geometry after factorization (row0, rows, col0, cols per block id), its
+  permutation, pivot types and compact upper factor (%.17g), read by
+  tests/cpp/test_cpp_surface.cc.
 
 Usage: python tests/golden/make_golden.py
 """
@@ -91,7 +96,23 @@ def main():
                       "upper_sum": float(np.triu(r.factors).sum())})
     with open(os.path.join(HERE, "ref_large.json"), "w") as fh:
         json.dump(large, fh)
-    print(f"wrote {len(names)} small cases and {len(large)} large cases")
+
+    geo_cases = [(40, 7, 777000 + 100 * 40 + 10 * 7 + 1), (60, 4, 777000 + 100 * 60 + 10 * 4)]
+    with open(os.path.join(HERE, "ref_geometry.txt"), "w") as fh:
+        fh.write(f"{len(geo_cases)}\n")
+        for n, b, seed in geo_cases:
+            a = port.random_symmetric(n, seed)
+            r = ref.factor(a, b)
+            nbk = (n + b - 1) // b
+            fh.write(f"{n} {b} {seed} {nbk * (nbk + 1) // 2}\n")
+            for g in r.geometry:
+                fh.write(" ".join(str(int(x)) for x in g) + "\n")
+            fh.write(" ".join(str(int(x)) for x in r.perm) + "\n")
+            fh.write(" ".join(str(int(x)) for x in r.pivot_types) + "\n")
+            up = np.triu(r.factors)
+            for i in range(n):
+                fh.write(" ".join(f"{x:.17g}" for x in up[i]) + "\n")
+    print(f"wrote {len(names)} small cases, {len(large)} large cases, {len(geo_cases)} geometry cases")
 
 
 if __name__ == "__main__":
