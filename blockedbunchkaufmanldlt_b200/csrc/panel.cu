@@ -34,10 +34,14 @@
 
 #include "bbk_internal.cuh"
 
+#ifndef BBK_PANEL_THREADS
+#define BBK_PANEL_THREADS 128
+#endif
+
 namespace bbk {
 namespace {
 
-constexpr int kThreads = 128;
+constexpr int kThreads = BBK_PANEL_THREADS;
 constexpr int kWarps = kThreads / 32;
 constexpr int kCols = 4;  // columns per thread: S <= kCols * kThreads
 constexpr int kMaxPollPerLane = 8;  // exchange records polled per lane (grid <= 256)
@@ -256,6 +260,24 @@ __device__ __forceinline__ double div_or_zero(double x, double den) {
   return den == 0.0 ? 0.0 : xdiv(x, den);
 }
 
+// sum_{q < count} c[q] * w(q) in ascending q, every product and sum rounded
+// separately (the reference's order).  The products do not depend on the
+// running sum, so they are issued eight at a time ahead of the serial adds.
+template <typename WGet>
+__device__ __forceinline__ double ordered_dot(const double* c, int count, WGet&& w) {
+  double acc = 0.0;
+  int q = 0;
+  for (; q + 8 <= count; q += 8) {
+    double m[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) m[u] = xmul(c[q + u], w(q + u));
+#pragma unroll
+    for (int u = 0; u < 8; ++u) acc = xadd(acc, m[u]);
+  }
+  for (; q < count; ++q) acc = xadd(acc, xmul(c[q], w(q)));
+  return acc;
+}
+
 __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
   extern __shared__ double dsm[];
   __shared__ double s_red_v[kWarps];
@@ -312,20 +334,57 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
   long long fix_src = 0;
   int ncand = 0;
 
+  // Next-row prefetch: the row update of pivot p issues the loads of row p+1
+  // (each thread keeps its own columns, j = lo + t + k*kThreads), so their
+  // HBM latency hides behind the rest of the step.  A prefetched entry can
+  // be stale only in a column that an interchange rewrote meanwhile: the
+  // last step's swap column (fix_col, read from the frozen row instead) and
+  // the swap column of the step before it (prev_swap, re-read once its
+  // write is visible).
+  double nav[kCols];
+  int nav_row = -1;
+  // the next row's coefficient column (rows q < n_old), loaded during the
+  // interchange phase when it has at most 2 * kThreads rows
+  double cpre[2] = {0.0, 0.0};
+  bool coef_pre = false;
+  int prev_swap = -1, last_swap = -1;
+
   while (p < P.nominal_end) {
     const int lp = p - kstart;
-    const int jbeg = max(lo, p);
     // ---- row update: W[p, j] = A[p, j] - sum_q U[q, p] W[q, j]
     // (CopyCurrentRowToWorkspace + UpdateCurrentRowInWorkspace, :122-162)
     double av[kCols];
+    const bool use_nav = nav_row == p;
 #pragma unroll
     for (int k = 0; k < kCols; ++k) {
-      const int j = jbeg + t + k * kThreads;
-      av[k] = j < hi ? ((j == fix_col) ? ldcg(P.a + fix_src) : ldcg(P.a + p * lda + j)) : 0.0;
+      const int j = lo + t + k * kThreads;
+      double v = 0.0;
+      if (j < hi && j >= p) {
+        if (j == fix_col)
+          v = ldcg(P.a + fix_src);
+        else if (use_nav && j != prev_swap)
+          v = nav[k];
+        else
+          v = ldcg(P.a + p * lda + j);
+      }
+      av[k] = v;
     }
+#pragma unroll
+    for (int k = 0; k < kCols; ++k) {
+      const int j = lo + t + k * kThreads;
+      nav[k] = (j < hi && j > p) ? ldcg(P.a + (p + 1) * lda + j) : 0.0;
+    }
+    nav_row = p + 1;
+    prev_swap = last_swap;
+    last_swap = -1;
     {
       const double* ucol = P.ucm + static_cast<size_t>(coef_src) * ldu;
-      for (int q = t; q < n_old; q += kThreads) coef[q] = ldcg(ucol + q);
+      if (coef_pre) {
+        if (t < n_old) coef[t] = cpre[0];
+        if (t + kThreads < n_old) coef[t + kThreads] = cpre[1];
+      } else {
+        for (int q = t; q < n_old; q += kThreads) coef[q] = ldcg(ucol + q);
+      }
       if (t == 0) {
         coef[n_old] = extra0;
         coef[n_old + 1] = extra1;
@@ -337,10 +396,9 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
     int best_j = INT_MAX;
 #pragma unroll
     for (int k = 0; k < kCols; ++k) {
-      const int j = jbeg + t + k * kThreads;
-      if (j < hi) {
-        double acc = 0.0;
-        for (int q = 0; q < lp; ++q) acc = xadd(acc, xmul(coef[q], wget(q, j)));
+      const int j = lo + t + k * kThreads;
+      if (j < hi && j >= p) {
+        const double acc = ordered_dot(coef, lp, [&](int q) { return wget(q, j); });
         const double wv = xsub(av[k], acc);
         wput(lp, j, wv);
         if (j > p) {
@@ -381,10 +439,11 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
       ++ncand;
       // ---- candidate column W(i, r) = A(i, r) - sum_q U[q, r] W[q, i]
       // (CopyCandidateToWorkspace + UpdateCandidateInWorkspace, :184-352)
+      double cv[kCols];
 #pragma unroll
       for (int k = 0; k < kCols; ++k) {
-        const int i = jbeg + t + k * kThreads;
-        av[k] = i < hi ? (i <= r ? ldcg(P.a + i * lda + r) : ldcg(P.a + r * lda + i)) : 0.0;
+        const int i = lo + t + k * kThreads;
+        cv[k] = (i < hi && i >= p) ? (i <= r ? ldcg(P.a + i * lda + r) : ldcg(P.a + r * lda + i)) : 0.0;
       }
       {
         const double* ucol = P.ucm + static_cast<size_t>(r) * ldu;
@@ -395,11 +454,10 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
       double sig = 0.0;
 #pragma unroll
       for (int k = 0; k < kCols; ++k) {
-        const int i = jbeg + t + k * kThreads;
-        if (i < hi) {
-          double acc = 0.0;
-          for (int q = 0; q < lp; ++q) acc = xadd(acc, xmul(coef[q], wget(q, i)));
-          const double v = xsub(av[k], acc);
+        const int i = lo + t + k * kThreads;
+        if (i < hi && i >= p) {
+          const double acc = ordered_dot(coef, lp, [&](int q) { return wget(q, i); });
+          const double v = xsub(cv[k], acc);
           wcs[i - lo] = v;
           if (i != r) {
             const double av2 = fabs(v);
@@ -525,7 +583,15 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
       if (p + 1 < r) {
         fix_col = r;
         fix_src = p * lda + (p + 1);  // new A[p+1, r] = old A[p, p+1]
+      } else {
+        // r == p+1: the next row is the old row p (its diagonal is old A[p, p])
+#pragma unroll
+        for (int k = 0; k < kCols; ++k) {
+          const int j = lo + t + k * kThreads;
+          nav[k] = (j < hi && j > p + 1) ? av[k] : ((j == p + 1 && j < hi) ? ldcg(P.a + p * lda + p) : 0.0);
+        }
       }
+      last_swap = r;
       p += 1;
     } else {
       // SwapTwoByTwoPivot (:403-412, :500-587) + ScaleTwoByTwoPivot (:658-704)
@@ -602,7 +668,14 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
         fix_col = r;
         fix_src = s * lda + (p + 2);  // new A[p+2, r] = old A[s, p+2]
       }
+      if (r != s) last_swap = r;
       p += 2;
+    }
+    coef_pre = n_old <= 2 * kThreads;
+    if (coef_pre) {
+      const double* ucol = P.ucm + static_cast<size_t>(coef_src) * ldu;
+      cpre[0] = t < n_old ? ldcg(ucol + t) : 0.0;
+      cpre[1] = t + kThreads < n_old ? ldcg(ucol + t + kThreads) : 0.0;
     }
     __syncthreads();
     lap(4);
