@@ -18,6 +18,7 @@
 // matrix only (the reference also fills the unused lower halves of its
 // diagonal blocks; nothing ever reads them).
 #include <algorithm>
+#include <cstdlib>
 
 #include "bbk_internal.cuh"
 
@@ -171,37 +172,57 @@ __device__ __forceinline__ void mma_16x8x8(double (&c)[4], const double (&a)[4],
       : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
-template <bool kAK, bool kVec>
-__device__ void mma_tile(const UpdArgs& U, double* smem, int I, int J) {
-  using Sm = MmaSmem<kAK>;
-  const int i0 = U.tile_i0 + I * kBM, j0 = U.tile_j0 + J * kBN;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int g = lane >> 2, tq = lane & 3;
-  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-  double acc[2][4][4];
-#pragma unroll
-  for (int a = 0; a < 2; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b)
-#pragma unroll
-      for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.0;
+__device__ __forceinline__ void mma_16x8x16(double (&c)[4], const double (&a)[8], const double (&b)[4]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, "
+      "{%4,%5,%6,%7,%8,%9,%10,%11}, {%12,%13,%14,%15}, {%0,%1,%2,%3};"
+      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]),
+        "d"(b[0]), "d"(b[1]), "d"(b[2]), "d"(b[3]));
+}
 
-  const int nchunks = (U.inner + kBK - 1) / kBK;
-  double* st0 = smem;
-  double* st1 = smem + Sm::kStage;
-  load_stage<kAK, kVec>(U, st0, st0 + Sm::kASize, i0, j0, 0);
-  for (int ch = 0; ch < nchunks; ++ch) {
-    double* cur = (ch & 1) ? st1 : st0;
-    if (ch + 1 < nchunks) {
-      double* nxt = (ch & 1) ? st0 : st1;
-      load_stage<kAK, kVec>(U, nxt, nxt + Sm::kASize, i0, j0, (ch + 1) * kBK);
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
+constexpr int kCPitch = kBM + 4;  // C tile staged in a free stage buffer
+static_assert(kBM * kCPitch <= MmaSmem<true>::kStage, "C tile must fit in one stage buffer");
+
+// C tile (rows i0.., cols j0..) -> shared memory, 16-byte cp.async chunks;
+// entries outside the trailing region are zero-filled and never written back.
+__device__ __forceinline__ void load_c_tile(const UpdArgs& U, double* cs, int i0, int j0) {
+  for (int c = threadIdx.x; c < kBM * (kBN / 2); c += kThreadsMma) {
+    const int ii = c / (kBN / 2), jj = (c % (kBN / 2)) * 2;
+    const int i = i0 + ii, j = j0 + jj;
+    const bool ok = i >= U.i_lo && i < U.i_hi && j + 1 < U.j_hi && j >= U.j_lo;
+    const double* src = ok ? U.c + static_cast<long long>(i) * U.ldc + j : U.c;
+    cp_async_16(&cs[ii * kCPitch + jj], src, ok ? 16 : 0);
+  }
+}
+
+template <bool kAK, bool K16>
+__device__ __forceinline__ void mma_chunk(double* as, double* bs, double (&acc)[2][4][4], int wm, int wn,
+                                          int g, int tq) {
+  using Sm = MmaSmem<kAK>;
+  if (K16) {
+    // m16n8k16 fragments: a_i at (g + 8(i%2), tq + 4(i/2)), b_i at (tq + 4i, g)
+#pragma unroll
+    for (int ks = 0; ks < kBK; ks += 16) {
+      double af[2][8], bf[4][4];
+#pragma unroll
+      for (int mt = 0; mt < 2; ++mt) {
+        const int r = wm + mt * 16 + g;
+#pragma unroll
+        for (int u = 0; u < 8; ++u) af[mt][u] = Sm::a_at(as, r + 8 * (u & 1), ks + tq + 4 * (u >> 1));
+      }
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) {
+        const int col = wn + nt * 8 + g;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) bf[nt][u] = bs[(ks + tq + 4 * u) * Sm::kBStride + col];
+      }
+#pragma unroll
+      for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) mma_16x8x16(acc[mt][nt], af[mt], bf[nt]);
     }
-    __syncthreads();
-    double* as = cur;
-    double* bs = cur + Sm::kASize;
+  } else {
 #pragma unroll
     for (int ks = 0; ks < kBK; ks += 8) {
       double af[2][4], bf[4][2];
@@ -224,47 +245,110 @@ __device__ void mma_tile(const UpdArgs& U, double* smem, int I, int J) {
 #pragma unroll
         for (int nt = 0; nt < 4; ++nt) mma_16x8x8(acc[mt][nt], af[mt], bf[nt]);
     }
-    __syncthreads();
-  }
-  // C -= acc on the valid part of the tile
-#pragma unroll
-  for (int mt = 0; mt < 2; ++mt) {
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int i = i0 + wm + mt * 16 + g + h * 8;
-      if (i < U.i_lo || i >= U.i_hi) continue;
-      double* crow = U.c + static_cast<long long>(i) * U.ldc;
-#pragma unroll
-      for (int nt = 0; nt < 4; ++nt) {
-        const int j = j0 + wn + nt * 8 + tq * 2;
-        const double v0 = acc[mt][nt][h * 2], v1 = acc[mt][nt][h * 2 + 1];
-        const bool ok0 = j >= U.j_lo && j < U.j_hi && (!U.upper_only || i <= j);
-        const bool ok1 = j + 1 >= U.j_lo && j + 1 < U.j_hi && (!U.upper_only || i <= j + 1);
-        if (kVec && ok0 && ok1) {
-          double2* p2 = reinterpret_cast<double2*>(crow + j);
-          double2 cv = *p2;
-          cv.x -= v0;
-          cv.y -= v1;
-          *p2 = cv;
-        } else {
-          if (ok0) crow[j] -= v0;
-          if (ok1) crow[j + 1] -= v1;
-        }
-      }
-    }
   }
 }
 
-template <bool kAK, bool kVec>
+// Persistent over tiles, double-buffered over K chunks.  At a tile's last
+// chunk the idle buffer receives the C tile (vector path), and right after
+// the last chunk's MMAs the buffer just freed receives the next tile's first
+// chunk, so neither latency sits on the critical path.
+template <bool kAK, bool kVec, bool K16>
 __global__ void __launch_bounds__(kThreadsMma) mma_update_kernel(UpdArgs U) {
+  using Sm = MmaSmem<kAK>;
   extern __shared__ double smem[];
   if (!resolve_range(U)) return;
   const int ntiles = tile_count(U);
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    int I, J;
-    tile_coords(U, t, I, J);
-    mma_tile<kAK, kVec>(U, smem, I, J);
+  int t = blockIdx.x;
+  if (t >= ntiles) return;
+  const int nchunks = (U.inner + kBK - 1) / kBK;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, tq = lane & 3;
+  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+  double* stage[2] = {smem, smem + Sm::kStage};
+
+  int I, J;
+  tile_coords(U, t, I, J);
+  int i0 = U.tile_i0 + I * kBM, j0 = U.tile_j0 + J * kBN;
+  load_stage<kAK, kVec>(U, stage[0], stage[0] + Sm::kASize, i0, j0, 0);
+  cp_async_commit();
+  int cur = 0;
+  for (;;) {
+    double acc[2][4][4];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.0;
+    for (int ch = 0; ch < nchunks; ++ch) {
+      const int nxt = cur ^ 1;
+      if (ch + 1 < nchunks) {
+        load_stage<kAK, kVec>(U, stage[nxt], stage[nxt] + Sm::kASize, i0, j0, (ch + 1) * kBK);
+        cp_async_commit();
+        cp_async_wait<1>();
+      } else if (kVec) {
+        load_c_tile(U, stage[nxt], i0, j0);
+        cp_async_commit();
+        cp_async_wait<1>();
+      } else {
+        cp_async_wait<0>();
+      }
+      __syncthreads();  // chunk ch is in stage[cur]
+      mma_chunk<kAK, K16>(stage[cur], stage[cur] + Sm::kASize, acc, wm, wn, g, tq);
+      __syncthreads();  // every warp is done with stage[cur]
+      if (ch + 1 < nchunks) cur = nxt;
+    }
+    // stage[cur] is free; stage[cur ^ 1] holds the C tile (vector path)
+    const int tn = t + static_cast<int>(gridDim.x);
+    int ni0 = 0, nj0 = 0;
+    if (tn < ntiles) {
+      int nI, nJ;
+      tile_coords(U, tn, nI, nJ);
+      ni0 = U.tile_i0 + nI * kBM;
+      nj0 = U.tile_j0 + nJ * kBN;
+      load_stage<kAK, kVec>(U, stage[cur], stage[cur] + Sm::kASize, ni0, nj0, 0);
+      cp_async_commit();
+      if (kVec) cp_async_wait<1>();
+    } else if (kVec) {
+      cp_async_wait<0>();
+    }
+    if (kVec) __syncthreads();  // C tile visible
+    const double* cs = stage[cur ^ 1];
+    // C -= acc on the valid part of the tile
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int ii = wm + mt * 16 + g + h * 8;
+        const int i = i0 + ii;
+        if (i < U.i_lo || i >= U.i_hi) continue;
+        double* crow = U.c + static_cast<long long>(i) * U.ldc;
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+          const int jj = wn + nt * 8 + tq * 2;
+          const int j = j0 + jj;
+          const double v0 = acc[mt][nt][h * 2], v1 = acc[mt][nt][h * 2 + 1];
+          const bool ok0 = j >= U.j_lo && j < U.j_hi && (!U.upper_only || i <= j);
+          const bool ok1 = j + 1 >= U.j_lo && j + 1 < U.j_hi && (!U.upper_only || i <= j + 1);
+          if (kVec && ok0 && ok1) {
+            double2 cv = *reinterpret_cast<const double2*>(cs + ii * kCPitch + jj);
+            cv.x -= v0;
+            cv.y -= v1;
+            *reinterpret_cast<double2*>(crow + j) = cv;
+          } else {
+            if (ok0) crow[j] -= v0;
+            if (ok1) crow[j + 1] -= v1;
+          }
+        }
+      }
+    }
+    if (tn >= ntiles) break;
+    __syncthreads();  // the C buffer becomes the next tile's second chunk buffer
+    t = tn;
+    i0 = ni0;
+    j0 = nj0;
   }
+  cp_async_wait<0>();
 }
 
 // ---------------------------------------------------------------------------
@@ -349,17 +433,23 @@ __global__ void __launch_bounds__(kThreadsSimt) simt_update_kernel(UpdArgs U) {
   }
 }
 
+// MMA shape of the tensor-core update: m16n8k8 by default; BBK_UPDATE_K16=1
+// selects m16n8k16 (tuning; the same speed on this part).
+bool use_k16() {
+  static const bool v = [] {
+    const char* e = getenv("BBK_UPDATE_K16");
+    return e ? atoi(e) != 0 : false;
+  }();
+  return v;
+}
+
 template <bool kAK, bool kVec>
 int launch_mma(const UpdArgs& U, int grid, cudaStream_t s) {
-  static bool configured = false;
   const size_t bytes = MmaSmem<kAK>::kBytes;
-  if (!configured) {
-    BBK_CUDA_TRY(cudaFuncSetAttribute(mma_update_kernel<kAK, kVec>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      static_cast<int>(bytes)));
-    configured = true;
-  }
-  mma_update_kernel<kAK, kVec><<<grid, kThreadsMma, bytes, s>>>(U);
+  auto fn = use_k16() ? mma_update_kernel<kAK, kVec, true> : mma_update_kernel<kAK, kVec, false>;
+  BBK_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(bytes)));
+  fn<<<grid, kThreadsMma, bytes, s>>>(U);
   BBK_CUDA_TRY(cudaGetLastError());
   count_launch();
   return BBK_OK;
