@@ -35,7 +35,12 @@ BBK_ERR_WORKSPACE = 8
 UPDATE_FP64 = 0
 UPDATE_FP64_ORDERED = 1
 UPDATE_FP32 = 2
-UPDATE_MODES = {"fp64": UPDATE_FP64, "fp64_ordered": UPDATE_FP64_ORDERED, "fp32": UPDATE_FP32}
+UPDATE_BF16 = 3
+UPDATE_BF16X3 = 4
+UPDATE_MODES = {"fp64": UPDATE_FP64, "fp64_ordered": UPDATE_FP64_ORDERED, "fp32": UPDATE_FP32,
+                "bf16": UPDATE_BF16, "bf16x3": UPDATE_BF16X3}
+REFINE_CLASSICAL = 0
+REFINE_GMRES = 1
 
 # Every symbol include/bbk_ldlt.h declares.
 EXPORTS = (
@@ -45,7 +50,15 @@ EXPORTS = (
     "bbk_solve_workspace_size", "bbk_solve_device", "bbk_solve_host", "bbk_factor_solve_host",
     "bbk_reconstruct_device", "bbk_scale_one_by_one", "bbk_scale_two_by_two",
     "bbk_update_trailing_block", "bbk_profile_begin", "bbk_profile_end", "bbk_panel_stats", "bbk_panel_stats_raw", "bbk_solve_device_noalloc",
+    "bbk_solve_refined_workspace_size", "bbk_solve_refined_device",
 )
+
+
+class RefineInfo(ctypes.Structure):
+    """bbk_refine_info"""
+    _fields_ = [("iterations", ctypes.c_int), ("inner_iterations", ctypes.c_int),
+                ("converged", ctypes.c_int), ("reserved", ctypes.c_int),
+                ("initial_backward_error", ctypes.c_double), ("backward_error", ctypes.c_double)]
 SOLVE_NOALLOC_MAX_ELEMENTS = 524288  # n * nrhs limit of bbk_solve_device_noalloc
 PROFILE_CLASSES = ("init", "panel", "finalize", "update", "solve")
 
@@ -112,6 +125,10 @@ def lib() -> ctypes.CDLL:
         "bbk_solve_device": ([_c_int, _vp, _c_ll, _vp, _vp, _c_int, _vp, _c_ll, _vp, _c_sz, _vp], _c_int),
         "bbk_solve_host": ([_c_int, _vp, _c_ll, _vp, _vp, _c_int, _vp, _c_ll], _c_int),
         "bbk_solve_device_noalloc": ([_c_int, _vp, _c_ll, _vp, _vp, _c_int, _vp, _c_ll, _vp], _c_int),
+        "bbk_solve_refined_workspace_size": ([_c_int, _c_int, _c_int], _c_sz),
+        "bbk_solve_refined_device": ([_c_int, _vp, _c_ll, _vp, _c_ll, _vp, _vp, _c_int, _vp, _c_ll, _vp,
+                                      _c_ll, ctypes.c_double, _c_int, _c_int, _c_int, _vp, _vp, _c_sz,
+                                      _vp], _c_int),
         "bbk_factor_solve_host": ([_c_int, _c_int, _vp, _c_ll, _vp, _vp, _vp, _c_int, _vp, _c_ll,
                                    _c_int], _c_int),
         "bbk_reconstruct_device": ([_c_int, _vp, _c_ll, _vp, _vp, _vp, _c_ll, _vp], _c_int),
@@ -246,6 +263,29 @@ def solve_device(f, perm, pivot_types, b, stream=None, workspace=None):
                                  nrhs, ctypes.c_void_p(b.data_ptr()), ldb, ws_ptr, ws_bytes,
                                  _stream_ptr(stream)))
     return b
+
+
+def solve_refined_device(a, f, perm, pivot_types, b, tol=1e-12, max_iter=30, method="gmres",
+                         restart=20, stream=None, workspace=None):
+    """FP64-refined solve on the device.  ``a`` is the original matrix (upper
+    triangle used), ``f`` the compact factors, ``b`` (nrhs, n) right-hand
+    sides.  Returns (x, RefineInfo)."""
+    import torch
+    n = f.shape[0]
+    bb = b if b.dim() == 2 else b.reshape(1, n)
+    x = torch.empty_like(bb)
+    info = RefineInfo()
+    meth = {"classical": REFINE_CLASSICAL, "gmres": REFINE_GMRES}[method] if isinstance(method, str) else method
+    ws_ptr, ws_bytes = (None, 0)
+    if workspace is not None:
+        ws_ptr, ws_bytes = ctypes.c_void_p(workspace.data_ptr()), workspace.numel() * workspace.element_size()
+    check(lib().bbk_solve_refined_device(n, ctypes.c_void_p(a.data_ptr()), a.stride(0),
+                                         ctypes.c_void_p(f.data_ptr()), f.stride(0),
+                                         ctypes.c_void_p(perm.data_ptr()), ctypes.c_void_p(pivot_types.data_ptr()),
+                                         bb.shape[0], ctypes.c_void_p(bb.data_ptr()), bb.stride(0),
+                                         ctypes.c_void_p(x.data_ptr()), x.stride(0), tol, max_iter, meth,
+                                         restart, ctypes.byref(info), ws_ptr, ws_bytes, _stream_ptr(stream)))
+    return (x if b.dim() == 2 else x.reshape(n)), info
 
 
 def reconstruct_device(f, perm, pivot_types, stream=None):

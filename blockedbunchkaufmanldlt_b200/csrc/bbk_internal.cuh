@@ -120,6 +120,11 @@ int solve_enqueue(int n, const double* f, long long ldf, const int* perm,
                   const int* pivot_types, int nrhs, double* b, long long ldb,
                   double* work, cudaStream_t s);
 size_t solve_work_doubles(int n, int nrhs);
+size_t refine_work_doubles(int n, int nrhs, int restart);
+int refine_enqueue(int n, const double* a, long long lda, const double* f, long long ldf,
+                   const int* perm, const int* pt, int nrhs, const double* b, double* x, double tol,
+                   int max_iter, int method, int restart, double* work, bbk_refine_info* info,
+                   cudaStream_t s);
 int reconstruct_enqueue(int n, const double* f, long long ldf, const int* perm,
                         const int* pivot_types, double* out, long long ldo,
                         double* work, cudaStream_t s);
@@ -148,5 +153,6 @@ struct FactorPlan {
   int grid = 0;              // CTAs of the panel kernel
   unsigned long long timeout_ns = 0;
   unsigned long long* stats = nullptr;  // optional per-phase panel timing
+  double* scales = nullptr;  // BF16 update: 2 x (n/64 + 2) power-of-two scales
 };
 }  // namespace bbk

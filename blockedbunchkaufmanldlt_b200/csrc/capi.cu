@@ -93,6 +93,7 @@ size_t carve_factor(FactorPlan& plan, char* base) {
   plan.uout = c.take<double>(static_cast<size_t>(b + 2) * plan.ldu);
   // candidate column (n) followed by the interchange staging area
   plan.wc = c.take<double>(static_cast<size_t>(npad) + 2 * align_up(static_cast<size_t>(b) + 4, 2));
+  plan.scales = c.take<double>(2 * (static_cast<size_t>(n) / 64 + 2));
   c.take<int>(4);  // status word for the synchronous entry point
   return c.off;
 }
@@ -108,7 +109,8 @@ int validate_factor_args(int n, int block_size, const double* a, long long lda, 
   if (lda < n) return set_error(BBK_ERR_INVALID_ARGUMENT, "lda (%lld) < n (%d)", lda, n);
   if (!a || !perm || !pivot_types)
     return set_error(BBK_ERR_INVALID_ARGUMENT, "null matrix, permutation or pivot array");
-  if (mode != BBK_UPDATE_FP64 && mode != BBK_UPDATE_FP64_ORDERED && mode != BBK_UPDATE_FP32)
+  if (mode != BBK_UPDATE_FP64 && mode != BBK_UPDATE_FP64_ORDERED && mode != BBK_UPDATE_FP32 &&
+      mode != BBK_UPDATE_BF16 && mode != BBK_UPDATE_BF16X3)
     return set_error(BBK_ERR_INVALID_ARGUMENT, "unknown update mode %d", mode);
   return BBK_OK;
 }
@@ -491,6 +493,72 @@ int bbk_factor_solve_host(int n, int block_size, double* a, long long lda, int* 
   if (h_status != BBK_OK)
     return set_error(h_status, "factorization aborted on the device: %s", bbk_status_string(h_status));
   return BBK_OK;
+}
+
+size_t bbk_solve_refined_workspace_size(int n, int nrhs, int restart) {
+  if (n <= 0 || nrhs <= 0 || restart < 0) return 0;
+  const size_t vec = static_cast<size_t>(n) * nrhs;
+  return (refine_work_doubles(n, nrhs, restart > 0 ? restart : 1) + 2 * vec) * sizeof(double) + kAlign;
+}
+
+int bbk_solve_refined_device(int n, const double* a, long long lda, const double* factors,
+                             long long ldf, const int* perm, const int* pivot_types, int nrhs,
+                             const double* b, long long ldb, double* x, long long ldx, double tol,
+                             int max_iter, int method, int restart, bbk_refine_info* info,
+                             void* workspace, size_t workspace_bytes, void* stream) {
+  int rc = validate_solve(n, factors, ldf, perm, pivot_types, nrhs, b, ldb);
+  if (rc) return rc;
+  if (!a || lda < n || !x || (nrhs > 0 && ldx < n) || !info)
+    return set_error(BBK_ERR_INVALID_ARGUMENT, "bad refinement arguments");
+  if (method != BBK_REFINE_CLASSICAL && method != BBK_REFINE_GMRES)
+    return set_error(BBK_ERR_INVALID_ARGUMENT, "unknown refinement method %d", method);
+  if (max_iter < 0 || !(tol >= 0.0) || (method == BBK_REFINE_GMRES && restart <= 0))
+    return set_error(BBK_ERR_INVALID_ARGUMENT, "bad refinement controls");
+  *info = bbk_refine_info{};
+  if (nrhs == 0) {
+    info->converged = 1;
+    return BBK_OK;
+  }
+  if ((rc = check_device())) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int m = method == BBK_REFINE_GMRES ? restart : 1;
+  const size_t need = bbk_solve_refined_workspace_size(n, nrhs, m);
+  char* base = static_cast<char*>(workspace);
+  bool owned = false;
+  if (base == nullptr) {
+    BBK_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&base), need, s));
+    owned = true;
+  } else if (workspace_bytes < need) {
+    return set_error(BBK_ERR_WORKSPACE, "refinement workspace needs %zu bytes, got %zu", need,
+                     workspace_bytes);
+  }
+  double* bc = reinterpret_cast<double*>(align_up(reinterpret_cast<uintptr_t>(base), kAlign));
+  const size_t vec = static_cast<size_t>(n) * nrhs;
+  double* xc = bc + vec;
+  double* work = xc + vec;
+  const size_t pitch_b = static_cast<size_t>(ldb) * sizeof(double);
+  const size_t pitch_x = static_cast<size_t>(ldx) * sizeof(double);
+  const size_t row = static_cast<size_t>(n) * sizeof(double);
+  cudaError_t err = cudaMemcpy2DAsync(bc, row, b, pitch_b, row, nrhs, cudaMemcpyDeviceToDevice, s);
+  if (err == cudaSuccess) err = cudaMemcpy2DAsync(xc, row, b, pitch_b, row, nrhs, cudaMemcpyDeviceToDevice, s);
+  if (err != cudaSuccess) {
+    rc = cuda_error(err, "refinement setup");
+  } else {
+    // x0 from the factors, then FP64 refinement (the solve scratch sits at
+    // the end of the refinement workspace)
+    rc = enqueue_solve(n, factors, ldf, perm, pivot_types, nrhs, xc, n,
+                       work + refine_work_doubles(n, nrhs, m) - solve_work_doubles(n, nrhs), s);
+    if (!rc)
+      rc = refine_enqueue(n, a, lda, factors, ldf, perm, pivot_types, nrhs, bc, xc, tol, max_iter,
+                          method, m, work, info, s);
+    if (!rc) {
+      err = cudaMemcpy2DAsync(x, pitch_x, xc, row, row, nrhs, cudaMemcpyDeviceToDevice, s);
+      if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+      if (err != cudaSuccess) rc = cuda_error(err, "refinement");
+    }
+  }
+  if (owned) cudaFreeAsync(base, s);
+  return rc;
 }
 
 int bbk_reconstruct_device(int n, const double* factors, long long ldf, const int* perm,

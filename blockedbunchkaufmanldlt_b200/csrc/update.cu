@@ -5,7 +5,7 @@
 // points (ScaleOneByOnePivot / ScaleTwoByTwoPivot / UpdateTrailingBlock).
 //
 // C(i,j) -= sum_k A(i,k) B(k,j) with A(i,k) = U[k, i] and B(k,j) = W[k, j].
-// Three arithmetics:
+// Arithmetics:
 //   FP64          FP64 tensor cores: mma.sync.m16n8k8.f64 from shared-memory
 //                 tiles staged with cp.async (double-buffered); 64x64 C tile
 //                 per CTA, 32x32 per warp.
@@ -14,11 +14,17 @@
 //                 reference's arithmetic.
 //   FP32          operands rounded to FP32, FP32 FMA accumulation, the result
 //                 subtracted in FP64.
+//   BF16, BF16X3  operands scaled by per-64-block powers of two and split
+//                 into one or three BF16 terms, mma.sync m16n8k16 BF16 with
+//                 FP32 accumulation, the result unscaled and subtracted in FP64.
 // In the factorization the C tiles cover the upper triangle of the trailing
 // matrix only (the reference also fills the unused lower halves of its
 // diagonal blocks; nothing ever reads them).
+#include <cuda_bf16.h>
+
 #include <algorithm>
 #include <cstdlib>
+#include <type_traits>
 
 #include "bbk_internal.cuh"
 
@@ -46,6 +52,9 @@ struct UpdArgs {
   const DeviceState* st;
   int panel;
   int n;
+  // BF16 mode: per 64-block power-of-two scales of A rows and B columns
+  const double* a_scale;
+  const double* b_scale;
 };
 
 __device__ __forceinline__ void cp_async_8(double* smem_dst, const double* gsrc, bool valid) {
@@ -196,6 +205,86 @@ __device__ __forceinline__ void load_c_tile(const UpdArgs& U, double* cs, int i0
   }
 }
 
+
+__device__ __forceinline__ void mma_bf16_16x8x16(float (&c)[4], const unsigned (&a)[4], const unsigned (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// Split of a (scaled) double into BF16 terms: x ~ t0 + t1 + t2, each term
+// the BF16 rounding of what the previous terms left over (kTerms = 1 is the
+// plain rounding).
+template <int kTerms>
+__device__ __forceinline__ void split_bf16(double x, float (&t)[3]) {
+  float rest = static_cast<float>(x);
+#pragma unroll
+  for (int k = 0; k < kTerms; ++k) {
+    t[k] = __bfloat162float(__float2bfloat16_rn(rest));
+    rest -= t[k];
+  }
+}
+
+__device__ __forceinline__ unsigned pack2(float lo, float hi) {
+  const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);  // exact: both are BF16 values
+  return *reinterpret_cast<const unsigned*>(&v);
+}
+
+// BF16 chunk: FP64 tile in shared memory, operands scaled by sa / sb and
+// split into kTerms BF16 terms while building fragments, FP32 accumulation.
+// With three terms the products t_i(a) t_j(b), i + j <= 2, are kept (six
+// MMAs per fragment pair), which carries about FP32 accuracy.
+//   A frag (16x16): a0,a1 (g, 2t..2t+1); a2,a3 (g+8, 2t..); a4,a5 (g, 2t+8..);
+//   a6,a7 (g+8, 2t+8..).  B frag (16x8): b0,b1 (2t..2t+1, g); b2,b3 (2t+8.., g).
+template <bool kAK, int kTerms>
+__device__ __forceinline__ void bf16_chunk(double* as, double* bs, float (&acc)[2][4][4], int wm, int wn,
+                                           int g, int tq, double sa, double sb) {
+  using Sm = MmaSmem<kAK>;
+#pragma unroll
+  for (int ks = 0; ks < kBK; ks += 16) {
+    unsigned af[kTerms][2][4], bf[kTerms][4][2];
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt) {
+      const int r = wm + mt * 16 + g;
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int rr = r + 8 * (u & 1), kk = ks + 2 * tq + 8 * (u >> 1);
+        float x0[3], x1[3];
+        split_bf16<kTerms>(Sm::a_at(as, rr, kk) * sa, x0);
+        split_bf16<kTerms>(Sm::a_at(as, rr, kk + 1) * sa, x1);
+#pragma unroll
+        for (int k = 0; k < kTerms; ++k) af[k][mt][u] = pack2(x0[k], x1[k]);
+      }
+    }
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) {
+      const int col = wn + nt * 8 + g;
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int kk = ks + 2 * tq + 8 * u;
+        float y0[3], y1[3];
+        split_bf16<kTerms>(bs[kk * Sm::kBStride + col] * sb, y0);
+        split_bf16<kTerms>(bs[(kk + 1) * Sm::kBStride + col] * sb, y1);
+#pragma unroll
+        for (int k = 0; k < kTerms; ++k) bf[k][nt][u] = pack2(y0[k], y1[k]);
+      }
+    }
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) {
+        // smallest products first
+#pragma unroll
+        for (int ia = kTerms - 1; ia >= 0; --ia)
+#pragma unroll
+          for (int ib = kTerms - 1; ib >= 0; --ib)
+            if (ia + ib <= kTerms - 1) mma_bf16_16x8x16(acc[mt][nt], af[ia][mt], bf[ib][nt]);
+      }
+  }
+}
+
 template <bool kAK, bool K16>
 __device__ __forceinline__ void mma_chunk(double* as, double* bs, double (&acc)[2][4][4], int wm, int wn,
                                           int g, int tq) {
@@ -252,9 +341,11 @@ __device__ __forceinline__ void mma_chunk(double* as, double* bs, double (&acc)[
 // chunk the idle buffer receives the C tile (vector path), and right after
 // the last chunk's MMAs the buffer just freed receives the next tile's first
 // chunk, so neither latency sits on the critical path.
-template <bool kAK, bool kVec, bool K16>
+template <bool kAK, bool kVec, bool K16, int kBf16Terms = 0>
 __global__ void __launch_bounds__(kThreadsMma) mma_update_kernel(UpdArgs U) {
   using Sm = MmaSmem<kAK>;
+  constexpr bool kBf16 = kBf16Terms > 0;
+  using Acc = typename std::conditional<kBf16, float, double>::type;
   extern __shared__ double smem[];
   if (!resolve_range(U)) return;
   const int ntiles = tile_count(U);
@@ -273,13 +364,18 @@ __global__ void __launch_bounds__(kThreadsMma) mma_update_kernel(UpdArgs U) {
   cp_async_commit();
   int cur = 0;
   for (;;) {
-    double acc[2][4][4];
+    Acc acc[2][4][4];
 #pragma unroll
     for (int a = 0; a < 2; ++a)
 #pragma unroll
       for (int b = 0; b < 4; ++b)
 #pragma unroll
-        for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.0;
+        for (int c = 0; c < 4; ++c) acc[a][b][c] = Acc(0);
+    double sa = 1.0, sb = 1.0;
+    if (kBf16) {
+      sa = U.a_scale[(i0 - U.tile_i0) / kBM];
+      sb = U.b_scale[(j0 - U.tile_j0) / kBN];
+    }
     for (int ch = 0; ch < nchunks; ++ch) {
       const int nxt = cur ^ 1;
       if (ch + 1 < nchunks) {
@@ -294,7 +390,11 @@ __global__ void __launch_bounds__(kThreadsMma) mma_update_kernel(UpdArgs U) {
         cp_async_wait<0>();
       }
       __syncthreads();  // chunk ch is in stage[cur]
-      mma_chunk<kAK, K16>(stage[cur], stage[cur] + Sm::kASize, acc, wm, wn, g, tq);
+      if constexpr (kBf16)
+        bf16_chunk<kAK, (kBf16Terms > 0 ? kBf16Terms : 1)>(stage[cur], stage[cur] + Sm::kASize, acc, wm,
+                                                          wn, g, tq, sa, sb);
+      else
+        mma_chunk<kAK, K16>(stage[cur], stage[cur] + Sm::kASize, acc, wm, wn, g, tq);
       __syncthreads();  // every warp is done with stage[cur]
       if (ch + 1 < nchunks) cur = nxt;
     }
@@ -327,7 +427,9 @@ __global__ void __launch_bounds__(kThreadsMma) mma_update_kernel(UpdArgs U) {
         for (int nt = 0; nt < 4; ++nt) {
           const int jj = wn + nt * 8 + tq * 2;
           const int j = j0 + jj;
-          const double v0 = acc[mt][nt][h * 2], v1 = acc[mt][nt][h * 2 + 1];
+          const double unscale = kBf16 ? 1.0 / (sa * sb) : 1.0;
+          const double v0 = static_cast<double>(acc[mt][nt][h * 2]) * unscale;
+          const double v1 = static_cast<double>(acc[mt][nt][h * 2 + 1]) * unscale;
           const bool ok0 = j >= U.j_lo && j < U.j_hi && (!U.upper_only || i <= j);
           const bool ok1 = j + 1 >= U.j_lo && j + 1 < U.j_hi && (!U.upper_only || i <= j + 1);
           if (kVec && ok0 && ok1) {
@@ -455,6 +557,8 @@ int launch_mma(const UpdArgs& U, int grid, cudaStream_t s) {
   return BBK_OK;
 }
 
+__global__ void block_scale_kernel(UpdArgs U, double* a_scale, double* b_scale);
+
 int launch_by_mode(const UpdArgs& U, int mode, bool ak, bool vec, int grid_mma, int grid_simt,
                    cudaStream_t s) {
   switch (mode) {
@@ -468,12 +572,63 @@ int launch_by_mode(const UpdArgs& U, int mode, bool ak, bool vec, int grid_mma, 
     case BBK_UPDATE_FP32:
       simt_update_kernel<float, false><<<grid_simt, kThreadsSimt, 0, s>>>(U);
       break;
+    case BBK_UPDATE_BF16:
+    case BBK_UPDATE_BF16X3: {
+      if (!(ak && vec) || U.a_scale == nullptr)
+        return set_error(BBK_ERR_INVALID_ARGUMENT, "BF16 update needs the factorization layout");
+      const int sms = device_sm_count();
+      block_scale_kernel<<<2 * sms, 256, 0, s>>>(U, const_cast<double*>(U.a_scale),
+                                                  const_cast<double*>(U.b_scale));
+      BBK_CUDA_TRY(cudaGetLastError());
+      count_launch();
+      const size_t bytes = MmaSmem<true>::kBytes;
+      auto fn = mode == BBK_UPDATE_BF16 ? mma_update_kernel<true, true, false, 1>
+                                        : mma_update_kernel<true, true, false, 3>;
+      BBK_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(bytes)));
+      fn<<<grid_mma, kThreadsMma, bytes, s>>>(U);
+      break;
+    }
     default:
       return set_error(BBK_ERR_INVALID_ARGUMENT, "unknown update mode %d", mode);
   }
   BBK_CUDA_TRY(cudaGetLastError());
   count_launch();
   return BBK_OK;
+}
+
+// Power-of-two scales for the BF16 update: for every 64-block of trailing
+// columns, 2^-e with 2^e >= max |entry| over the panel's U rows (a_scale) and
+// W rows (b_scale), so the scaled operands have magnitude <= 1.
+__global__ void block_scale_kernel(UpdArgs U, double* a_scale, double* b_scale) {
+  if (!resolve_range(U)) return;
+  const int nblk = U.tiles_m;
+  for (int blk = blockIdx.x; blk < 2 * nblk; blk += gridDim.x) {
+    const bool is_a = blk < nblk;
+    const int bi = is_a ? blk : blk - nblk;
+    const int c0 = U.tile_i0 + bi * kBM;
+    double m = 0.0;
+    for (int idx = threadIdx.x; idx < kBM * U.inner; idx += blockDim.x) {
+      const int cc = c0 + idx % kBM, k = idx / kBM;
+      if (cc < U.i_lo || cc >= U.n) continue;
+      const double v = is_a ? U.a[static_cast<long long>(cc) * U.a_si + k]
+                            : U.b[static_cast<long long>(k) * U.b_sk + cc];
+      m = fmax(m, fabs(v));
+    }
+    for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, off));
+    __shared__ double red[8];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int w = 1; w < static_cast<int>(blockDim.x >> 5); ++w) m = fmax(m, red[w]);
+      m = fmax(m, red[0]);
+      int e = 0;
+      frexp(m, &e);  // m = f * 2^e, 0.5 <= f < 1
+      const double sc = (m > 0.0 && isfinite(m)) ? ldexp(1.0, -e) : 1.0;
+      (is_a ? a_scale : b_scale)[bi] = sc;
+    }
+    __syncthreads();
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -519,6 +674,8 @@ int launch_update(const FactorPlan& plan, int panel, cudaStream_t s) {
   U.st = plan.state;
   U.panel = panel;
   U.n = plan.n;
+  U.a_scale = plan.scales;
+  U.b_scale = plan.scales ? plan.scales + (plan.n / kBM + 2) : nullptr;
   const int sms = device_sm_count();
   // tiles of the first trailing panel bound the work; persistent grid
   const long long nominal_e = std::max(0LL, static_cast<long long>(panel + 1) * plan.b - 1);

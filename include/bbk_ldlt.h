@@ -53,8 +53,14 @@ typedef enum bbk_update_mode {
   BBK_UPDATE_FP64 = 0,         /* FP64 tensor cores (DMMA mma.sync f64) */
   BBK_UPDATE_FP64_ORDERED = 1, /* FP64, reference summation order: bitwise
                                   identical to the reference */
-  BBK_UPDATE_FP32 = 2          /* operands rounded to FP32, FP32 accumulate,
+  BBK_UPDATE_FP32 = 2,         /* operands rounded to FP32, FP32 accumulate,
                                   result subtracted in FP64 */
+  BBK_UPDATE_BF16 = 3,         /* operands scaled by per-64-block powers of two
+                                  and rounded to BF16, FP32 accumulation on
+                                  tensor cores, result subtracted in FP64 */
+  BBK_UPDATE_BF16X3 = 4        /* as BF16, each operand split into three BF16
+                                  terms (six products): about FP32 accuracy
+                                  at BF16 tensor-core rates */
 } bbk_update_mode;
 
 /* ---- version / diagnostics ------------------------------------------- */
@@ -166,6 +172,39 @@ int bbk_solve_host(int n, const double* factors, long long ldf,
 int bbk_solve_device_noalloc(int n, const double* factors, long long ldf,
                              const int* perm, const int* pivot_types,
                              int nrhs, double* b, long long ldb,
+                             void* stream);
+
+/* ---- FP64 iterative refinement (no reference counterpart) -------------
+ * Solves A X = B with factors that may come from a low-precision update
+ * (BBK_UPDATE_FP32 / BBK_UPDATE_BF16), refining in FP64 against the original
+ * matrix `a` (upper triangle, lda) until every right-hand side's backward
+ * error ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf) <= tol or
+ * max_iter outer steps.  method BBK_REFINE_CLASSICAL: x += (LDL^T)^{-1} r;
+ * BBK_REFINE_GMRES: restarted FGMRES(restart) on the correction equation,
+ * right-preconditioned by the factors (for factor error x condition number
+ * too large for classical refinement).  Device pointers; b and x are
+ * column-major (b[c*ldb + i]).  `workspace` may be NULL (allocated with
+ * cudaMallocAsync), else bbk_solve_refined_workspace_size bytes. */
+typedef struct bbk_refine_info {
+  int iterations;                /* outer refinement steps */
+  int inner_iterations;          /* preconditioner applications */
+  int converged;                 /* 1 when backward_error <= tol */
+  int reserved;
+  double initial_backward_error; /* of the unrefined solution */
+  double backward_error;         /* final, max over right-hand sides */
+} bbk_refine_info;
+
+#define BBK_REFINE_CLASSICAL 0
+#define BBK_REFINE_GMRES 1
+
+size_t bbk_solve_refined_workspace_size(int n, int nrhs, int restart);
+int bbk_solve_refined_device(int n, const double* a, long long lda,
+                             const double* factors, long long ldf,
+                             const int* perm, const int* pivot_types, int nrhs,
+                             const double* b, long long ldb, double* x,
+                             long long ldx, double tol, int max_iter,
+                             int method, int restart, bbk_refine_info* info,
+                             void* workspace, size_t workspace_bytes,
                              void* stream);
 
 /* ---- factor + solve in one call, host buffers (the end-to-end path) ----

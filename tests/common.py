@@ -84,3 +84,25 @@ def kkt_matrix(n: int, h: int, seed: int, ridge: float = 1e-2) -> np.ndarray:
     a[h:, :h] = bm
     a[:h, h:] = bm.T
     return a
+
+
+def spectral_matrix(n: int, seed: int, lo: float = 1e-4, hi: float = 1e4) -> np.ndarray:
+    """A = Q diag(lam) Q^T with Q from the QR of a Gaussian matrix, |lam|
+    log-uniform in [lo, hi] and half of the signs negative (condition number
+    about hi/lo): the structure of the mixed-precision workload."""
+    rng = np.random.default_rng(seed)
+    q, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    mag = np.exp(rng.uniform(np.log(lo), np.log(hi), n))
+    sign = np.ones(n)
+    sign[rng.permutation(n)[: n // 2]] = -1.0
+    a = (q * (sign * mag)) @ q.T
+    return (a + a.T) / 2
+
+
+def backward_error(a: np.ndarray, x: np.ndarray, b: np.ndarray) -> float:
+    """max over columns of ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf)."""
+    x = x.reshape(a.shape[0], -1)
+    b = b.reshape(a.shape[0], -1)
+    r = b - a @ x
+    an = np.abs(a).sum(1).max()
+    return float(np.max(np.abs(r).max(0) / (an * np.abs(x).max(0) + np.abs(b).max(0))))
