@@ -54,6 +54,9 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU baseline sample time")
+    ap.add_argument("--workload", default="kkt", choices=["kkt", "mixed"],
+                    help="kkt: the headline FP64 factor+solve line; mixed: FP64 vs low-precision "
+                         "updates + FP64 refinement on an ill-conditioned matrix (n=20000, 16 RHS)")
     return ap.parse_args()
 
 
@@ -197,13 +200,13 @@ def update_flops(n: int, panel_end) -> float:
 
 
 def panel_bytes(n: int, panel_end) -> float:
-    """Lower bound on the panel kernels' traffic: per pivot p (local index lp)
-    the row update reads lp workspace rows and the matrix row over n - p
-    columns and writes the workspace row and the factor row."""
+    """Compulsory DRAM bytes of the panel launches: each panel of width w
+    starting at row k0 reads its w x (n - k0) strip of the matrix and writes
+    the workspace rows W and the compact factor rows of the same shape
+    (3 x 8 bytes per strip entry)."""
     b, k0 = 0.0, 0
     for e in panel_end:
-        for p in range(k0, e):
-            b += 8.0 * (n - p) * ((p - k0) + 3)
+        b += 24.0 * (e - k0) * (n - k0)
         k0 = e
     return b
 
@@ -326,13 +329,25 @@ def run_b200(args):
         v["share"] = (v["ms"] / total_prof) if total_prof > 0 else None
     dom = max(("trailing_update", "panel"), key=lambda k: kernels.get(k, {}).get("ms", 0.0))
     dk = kernels[dom]
+    # DRAM bytes per launch: the measured bytes per unit (profiles/traffic.json,
+    # from an ncu capture of this workload) times the units of an average
+    # launch of this run
     traffic = None
     traffic_path = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(traffic_path):
+    if os.path.exists(traffic_path) and dk.get("launches"):
         try:
             with open(traffic_path) as fh:
-                traffic = json.load(fh).get(dom)
-        except (OSError, ValueError):
+                per_unit = float(json.load(fh)[dom]["bytes_per_unit"])
+            if dom == "panel":
+                units, k0 = 0.0, 0
+                for e in pe_h:
+                    units += float(e - k0) * (n - k0)
+                    k0 = e
+                units *= args.steps
+            else:
+                units = upd_flops
+            traffic = per_unit * units / dk["launches"]
+        except (OSError, ValueError, KeyError):
             traffic = None
     roofline = {"kernel": dom, "bound": dk["bound"], "achieved": dk["achieved"], "peak": dk["peak"],
                 "unit": dk["unit"], "frac": dk["frac"], "traffic": traffic, "peak_source": dk["peak_source"]}
@@ -479,10 +494,96 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def spectral_device(n: int, seed: int, device, lo=1e-4, hi=1e4):
+    """A = Q diag(lam) Q^T, Q from the QR of a Gaussian matrix, |lam|
+    log-uniform in [lo, hi], half the signs negative (condition ~ hi/lo)."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    q, _ = torch.linalg.qr(torch.randn(n, n, generator=g, dtype=torch.float64, device=device))
+    mag = torch.exp(torch.empty(n, dtype=torch.float64, device=device).uniform_(
+        float(torch.log(torch.tensor(lo))), float(torch.log(torch.tensor(hi))), generator=g))
+    sign = torch.ones(n, dtype=torch.float64, device=device)
+    sign[torch.randperm(n, generator=g, device=device)[: n // 2]] = -1.0
+    a = (q * (sign * mag)) @ q.T
+    del q
+    a = (a + a.T) * 0.5
+    rhs = torch.randn(16, n, generator=g, dtype=torch.float64, device=device)
+    return a, rhs
+
+
+def run_mixed(args):
+    """FP64 path vs low-precision trailing updates + FP64 GMRES-IR: time to a
+    solution with backward error <= 1e-12 (every one of 16 right-hand sides),
+    and the forward error against the FP64 path's solution."""
+    import torch
+
+    import blockedbunchkaufmanldlt_b200 as bbk
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(0)
+    n = args.n if args.n != 10000 else 20000
+    blk = args.block
+    a0, rhs = spectral_device(n, args.seed, dev)
+    tol = 1e-12
+
+    def berr(x):
+        r = rhs.T - a0 @ x.T
+        return float((r.abs().amax(0) / (a0.abs().sum(1).amax() * x.T.abs().amax(0) + rhs.T.abs().amax(0))).max())
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record()
+        out = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return out, max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3)
+
+    results = {}
+    # FP64: factor + solve (+ FP64 refinement only if the plain solve misses tol)
+    for _ in range(1 + max(0, min(args.warmup, 1))):
+        w = a0.clone()
+
+        def fp64_path():
+            perm, pt, _ = bbk.factor_device(w, blk, mode="fp64")
+            x = rhs.clone()
+            bbk.solve_device(w, perm, pt, x)
+            return x, perm, pt
+        (x64, perm64, pt64), ms = timed(fp64_path)
+    e64 = berr(x64)
+    results["fp64"] = {"ms": ms, "backward_error": e64, "refine_steps": 0}
+    for mode in ("fp32", "bf16x3"):
+        for _ in range(1 + max(0, min(args.warmup, 1))):
+            w = a0.clone()
+
+            def mixed_path():
+                perm, pt, _ = bbk.factor_device(w, blk, mode=mode)
+                x, info = bbk.solve_refined_device(a0, w, perm, pt, rhs, tol=tol, max_iter=3,
+                                                   method="gmres", restart=50)
+                return x, info
+            (x, info), ms = timed(mixed_path)
+        fe = float((x - x64).abs().amax() / x64.abs().amax())
+        results[mode] = {"ms": ms, "backward_error": berr(x), "initial_backward_error": info.initial_backward_error,
+                         "refine_steps": info.iterations,
+                         "gmres_steps": info.inner_iterations, "converged": bool(info.converged),
+                         "forward_error_vs_fp64": fe, "speedup_vs_fp64": results["fp64"]["ms"] / ms}
+    line = {"metric": "time to backward error <= 1e-12, FP64 vs low-precision update + FP64 GMRES-IR",
+            "unit": "ms", "higher_is_better": False, "n_gpus": 1, "dtype": "f64 (panel, residual) + update",
+            "data": "synthetic: A = Q diag(lam) Q^T, Q from QR of a seeded Gaussian, |lam| log-uniform "
+                    "[1e-4, 1e4], half negative; 16 RHS N(0,1)",
+            "config": {"workload": f"mixed precision, n={n}, block {blk}, 16 RHS, condition ~1e8",
+                       "n": n, "block_size": blk, "nrhs": 16},
+            "results": results}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "mixed":
+        run_mixed(args)
     else:
         run_b200(args)
 
