@@ -75,6 +75,7 @@ struct DeviceState {
                   // its end (= start of P + 1) into kstart[(P + 1) & 1]
   int abort;      // nonzero: a kernel gave up; every later kernel returns
   int status;     // bbk_status of the factorization
+  int moved[2];   // panel P: count of indices its interchanges moved, in moved[P & 1]
 };
 
 // ---------------------------------------------------------------------------
@@ -142,12 +143,19 @@ struct FactorPlan {
   int* pivot_types = nullptr;
   int* panel_end = nullptr;  // may be null
   // workspace
-  double* w = nullptr;       // (b+1) rows x ldw: the panel's W rows
+  double* w = nullptr;       // (b+2) rows x ldw: the panel's W rows, final column order
   long long ldw = 0;
-  double* ucm = nullptr;     // n x ldu column-major copy of the panel's U rows
+  double* ucm = nullptr;     // n x ldu column-major U rows of the panel, final column order
   int ldu = 0;
-  double* uout = nullptr;    // (b+1) x ldu: final columns of the panel's pivots
-  double* wc = nullptr;      // n: candidate column
+  double* uslot = nullptr;   // n x ldu: U by column slot while the panel runs
+  double* wslot = nullptr;   // (b+2) x ldw: W by slot when shared memory cannot hold it
+  double* dlog = nullptr;    // 2 x (b+2): D entries of the panel's pivots
+  int* srcmap = nullptr;     // n: slot holding each index at the end of a panel
+  int* moved = nullptr;      // 2 x move_cap: indices a panel's interchanges moved
+  int move_cap = 0;
+  double* gbuf = nullptr;    // move_cap x ldw: gathered rows of the moved indices
+  double* gbuf2 = nullptr;   // n x move_cap: factored rows at the moved columns
+  int* permbuf = nullptr;    // move_cap: gathered permutation entries
   unsigned long long* slots = nullptr;  // 2 x grid x kSlotWords
   DeviceState* state = nullptr;
   int grid = 0;              // CTAs of the panel kernel

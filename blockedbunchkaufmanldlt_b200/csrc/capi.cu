@@ -90,9 +90,16 @@ size_t carve_factor(FactorPlan& plan, char* base) {
   plan.slots = c.take<unsigned long long>(2ull * kMaxPanelGrid * kSlotWords);
   plan.w = c.take<double>(static_cast<size_t>(b + 2) * npad);
   plan.ucm = c.take<double>(static_cast<size_t>(npad) * plan.ldu);
-  plan.uout = c.take<double>(static_cast<size_t>(b + 2) * plan.ldu);
-  // candidate column (n) followed by the interchange staging area
-  plan.wc = c.take<double>(static_cast<size_t>(npad) + 2 * align_up(static_cast<size_t>(b) + 4, 2));
+  plan.uslot = c.take<double>(static_cast<size_t>(npad) * plan.ldu);
+  plan.wslot = c.take<double>(static_cast<size_t>(b + 2) * npad);
+  plan.dlog = c.take<double>(2 * static_cast<size_t>(b + 2));
+  plan.srcmap = c.take<int>(static_cast<size_t>(npad));
+  // each pivot step moves at most two indices
+  plan.move_cap = static_cast<int>(align_up(2 * static_cast<size_t>(b) + 4, 4));
+  plan.moved = c.take<int>(2 * static_cast<size_t>(plan.move_cap));
+  plan.gbuf = c.take<double>(static_cast<size_t>(plan.move_cap) * npad);
+  plan.gbuf2 = c.take<double>(static_cast<size_t>(npad) * plan.move_cap);
+  plan.permbuf = c.take<int>(static_cast<size_t>(plan.move_cap));
   plan.scales = c.take<double>(2 * (static_cast<size_t>(n) / 64 + 2));
   c.take<int>(4);  // status word for the synchronous entry point
   return c.off;

@@ -1,6 +1,6 @@
 // Panel factorization of the blocked Bunch-Kaufman LDL^T: one persistent
 // cooperative launch per panel runs the panel's sequential pivot chain with
-// all CTAs, each owning a contiguous slice of the active columns [k0, n).
+// all CTAs, each owning a contiguous range of column slots.
 //
 // Follows BlockLdltDecomposition::FactorPanel and its helpers
 // (src/block_ldlt_decomposition.cc:80-704 in wentianshu/BlockedBunchKaufmanLDLT)
@@ -8,26 +8,31 @@
 // bitwise identical to the reference (every product and sum separately
 // rounded; this file is also compiled with --fmad=false).
 //
-// Data during a panel whose first row is k0 (lp = p - k0 is the local pivot):
-//   A    n x lda row-major upper: rows >= p are the partially updated matrix;
-//        the panel's own rows stay frozen until finalize_kernel writes the
-//        compact factor rows into them.
-//   W    row lp holds the workspace row W[p, j] (j >= p) of pivot p.
-//   Ucm  column-major U: Ucm[j*ldu + lp] = U[p, j].  Column j belongs to the
-//        CTA that owns column j, so U[., r] is one contiguous read.
-//   Uout the final compact column of each pivot column of the panel
-//        (rows < lp from Ucm after the last interchange touching it, then D).
-//   wc   the candidate column W(i, r), i >= p.
+// Slots.  Every active index x >= k0 (k0 = the panel's first row) owns a
+// slot: the physical row/column of A that holds its data, plus that slot's
+// workspace column W[., slot], U column Uslot[slot, .] and candidate value.
+// A symmetric interchange p <-> r (SwapOneByOnePivot / SwapTwoByTwoPivot,
+// :392-587) only exchanges the slots of p and r in two small maps that every
+// CTA updates identically: the window map (slot of each of the panel's rows)
+// and the CTA's own slot -> index map.  No data moves while the panel runs,
+// A is never written by this kernel, and the only values other CTAs read
+// from global memory are U columns written at least one exchange earlier.
+//
+// Data during a panel:
+//   shared   the CTA's slice of the panel rows: row m starts as
+//            A[k0 + m, slot] (loaded once) and becomes W[k0 + m, slot] when
+//            pivot row m is updated; the candidate column; the maps.
+//   Uslot    U[q, x] at Uslot[slot(x) * ldu + q].
+//   dlog     D of every pivot; ptype.
+// At the end the CTAs write W and U in final column order, publish the slot
+// of every index, and gather the rows of the moved indices (and the
+// factored rows' entries at the moved columns) into staging buffers.
+// finalize_kernel then writes the interchanged entries back, the
+// permutation, and the panel's compact factor rows.
 //
 // Per pivot step the grid meets once (no candidate) or twice (candidate
-// column needed).  Between one step's interchange/scaling phase and the next
-// step's row update there is no grid barrier: every write of the scaling phase
-// goes to a column its writer owns, except three kinds of value that the
-// next row update needs from other columns -- the next coefficients U[p, p']
-// (recomputed redundantly by every CTA from published scalars), the single
-// moved entry A[p', r] (read from the frozen row p instead), and a swapped
-// Ucm column (read from its pre-swap location).  Everything else is read
-// only after the next exchange.
+// column needed), in a tagged-record exchange that is also the argmax
+// reduction.
 #include <climits>
 #include <cstdio>
 #include <cstdlib>
@@ -43,23 +48,33 @@ namespace {
 
 constexpr int kThreads = BBK_PANEL_THREADS;
 constexpr int kWarps = kThreads / 32;
-constexpr int kCols = 4;  // columns per thread: S <= kCols * kThreads
+constexpr int kCols = 4;  // slots per thread: S <= kCols * kThreads
 constexpr int kMaxPollPerLane = 8;  // exchange records polled per lane (grid <= 256)
+constexpr int kRecBase = 4;  // record words before the published doubles: idx, hi, lo, slot
+static_assert(kRecBase + 2 * kMaxPub <= kSlotWords, "record too large");
 
 struct PanelArgs {
   int n;
   int panel;
   int nominal_end;  // min((panel+1)*b, n)
   int can_shift;    // another panel follows
+  int win_rows;     // b + 2: panel rows staged per slot
+  int win_pad;      // ints reserved for the window map
   double* a;
   long long lda;
-  double* w;
+  double* w;         // W rows, final column order (for the trailing update)
   long long ldw;
-  double* ucm;
+  double* wslot;     // W rows by slot when shared memory cannot hold them
+  double* uslot;     // U by slot
+  double* ucm;       // U, final column order: ucm[x * ldu + q]
   int ldu;
-  double* uout;
-  double* wc;
-  double* wstage;    // 2 x coef_cap: W columns p and p+1 for an interchange
+  double* dlog;      // dlog[2l] = D(l, l); dlog[2l+1] = D(l, l+1) of a 2x2
+  int* srcmap;       // slot of index x at the end of the panel
+  int* moved;        // 2 x move_cap
+  int move_cap;
+  double* gbuf;      // move_cap x ldw
+  double* gbuf2;     // n x move_cap
+  int* permbuf;
   int* perm;
   int* ptype;
   int* panel_end;
@@ -70,7 +85,7 @@ struct PanelArgs {
   unsigned tag_base;
   unsigned long long timeout_ns;
   int coef_cap;      // doubles reserved for the coefficient column
-  int w_smem;        // keep this CTA's workspace slice in shared memory
+  int w_smem;        // keep this CTA's panel rows in shared memory
   int smem_cols;     // slice width the shared-memory allocation holds
   unsigned long long* stats;  // optional per-phase nanoseconds (CTA 0)
   unsigned long long* pub_ts; // with stats: each CTA's publish timestamp
@@ -80,6 +95,7 @@ struct PanelArgs {
 struct ExchangeOut {
   double val;
   int idx;
+  int slot;
   int ok;
   double pub[kMaxPub];
 };
@@ -96,31 +112,41 @@ __device__ __forceinline__ double join_hi_lo(unsigned long long hi, unsigned lon
 
 // Argmax combine with the reference's tie rule (src/block_ldlt_decomposition.cc:
 // 164-182 scans ascending columns with a strict '>'): larger value wins, equal
-// values keep the lower index.  NaN never enters (callers skip it).
-__device__ __forceinline__ void argmax_join(double& v, int& i, double v2, int i2) {
+// values keep the lower index.  The slot travels with its index.  NaN never
+// enters (callers skip it).
+__device__ __forceinline__ void argmax_join(double& v, int& i, int& s, double v2, int i2, int s2) {
   if (v2 > v || (v2 == v && i2 < i)) {
     v = v2;
     i = i2;
+    s = s2;
   }
 }
 
-// CTA-collective: reduce (my_val, my_idx) over the CTA, publish the CTA's
-// record (reduction + its kMaxPub scalars in pub_in), wait for the records of
-// all `nslots` CTAs, and return the grid-wide argmax plus pub[k] taken from
-// the record of CTA pub_owner[k].  Must be called by every thread.
-__device__ void exchange(const PanelArgs& P, unsigned tag, double my_val, int my_idx,
-                         const double* pub_in, const int* pub_owner, int npub,
-                         double* s_red_v, int* s_red_i, ExchangeOut* out) {
+__device__ __forceinline__ void cp_async_8(double* smem_dst, const double* gsrc) {
+  const unsigned saddr = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(saddr), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// CTA-collective: reduce (my_val, my_idx, my_slot) over the CTA, publish the
+// CTA's record (reduction + its kMaxPub scalars in pub_in), wait for the
+// records of all `nslots` CTAs, and return the grid-wide argmax plus pub[k]
+// taken from the record of CTA pub_owner[k].  Must be called by every thread.
+__device__ void exchange(const PanelArgs& P, unsigned tag, double my_val, int my_idx, int my_slot,
+                         const double* pub_in, const int* pub_owner, int npub, double* s_red_v,
+                         int* s_red_i, int* s_red_s, ExchangeOut* out) {
   const int t = threadIdx.x;
   const int lane = t & 31, warp = t >> 5;
   for (int off = 16; off > 0; off >>= 1) {
     const double v2 = __shfl_down_sync(0xffffffffu, my_val, off);
     const int i2 = __shfl_down_sync(0xffffffffu, my_idx, off);
-    argmax_join(my_val, my_idx, v2, i2);
+    const int s2 = __shfl_down_sync(0xffffffffu, my_slot, off);
+    argmax_join(my_val, my_idx, my_slot, v2, i2, s2);
   }
   if (lane == 0) {
     s_red_v[warp] = my_val;
     s_red_i[warp] = my_idx;
+    s_red_s[warp] = my_slot;
   }
   __syncthreads();  // also orders this CTA's global writes before the fences
   // Structure-of-arrays records: word w of CTA c lives at
@@ -130,17 +156,19 @@ __device__ void exchange(const PanelArgs& P, unsigned tag, double my_val, int my
       P.slots + static_cast<size_t>(tag & 1u) * kSlotWords * P.slot_stride;
   if (warp == 0) {
     double v = s_red_v[0];
-    int i = s_red_i[0];
-    for (int k = 1; k < kWarps; ++k) argmax_join(v, i, s_red_v[k], s_red_i[k]);
-    // one record word per lane: (tag | idx), (tag | hi v), (tag | lo v), pubs
-    if (lane < 3 + 2 * npub) {
+    int i = s_red_i[0], sl = s_red_s[0];
+    for (int k = 1; k < kWarps; ++k) argmax_join(v, i, sl, s_red_v[k], s_red_i[k], s_red_s[k]);
+    // one record word per lane: (tag | idx), (tag | hi v), (tag | lo v), (tag | slot), pubs
+    if (lane < kRecBase + 2 * npub) {
       unsigned word;
       if (lane == 0) {
         word = static_cast<unsigned>(i);
+      } else if (lane == 3) {
+        word = static_cast<unsigned>(sl);
       } else {
-        const double x = lane < 3 ? v : pub_in[(lane - 3) >> 1];
+        const double x = lane < 3 ? v : pub_in[(lane - kRecBase) >> 1];
         const unsigned long long bits = static_cast<unsigned long long>(__double_as_longlong(x));
-        const bool high = lane < 3 ? lane == 1 : ((lane - 3) & 1) == 0;
+        const bool high = lane < 3 ? lane == 1 : ((lane - kRecBase) & 1) == 0;
         word = high ? static_cast<unsigned>(bits >> 32) : static_cast<unsigned>(bits);
       }
       if (P.pub_ts && lane == 0) P.pub_ts[blockIdx.x] = globaltimer_ns();
@@ -155,13 +183,13 @@ __device__ void exchange(const PanelArgs& P, unsigned tag, double my_val, int my
     // after the last record lands.
     const size_t st = P.slot_stride;
     const unsigned long long* src[kMaxPollPerLane];
-    unsigned long long wv[kMaxPollPerLane][3];
+    unsigned long long wv[kMaxPollPerLane][kRecBase];
     int nmine = 0;
     for (int sidx = lane; sidx < P.nslots && nmine < kMaxPollPerLane; sidx += 32)
       src[nmine++] = par_base + sidx;
     const bool has_pub = lane < npub;
     const unsigned long long* psrc =
-        has_pub ? par_base + static_cast<size_t>(3 + 2 * lane) * st + pub_owner[lane] : par_base;
+        has_pub ? par_base + static_cast<size_t>(kRecBase + 2 * lane) * st + pub_owner[lane] : par_base;
     unsigned pending = (1u << nmine) - 1u;
     bool pub_pending = has_pub;
     unsigned long long pw0 = 0, pw1 = 0;
@@ -171,9 +199,8 @@ __device__ void exchange(const PanelArgs& P, unsigned tag, double my_val, int my
 #pragma unroll
       for (int k = 0; k < kMaxPollPerLane; ++k) {
         if (pending & (1u << k)) {
-          wv[k][0] = ld_relaxed_u64(src[k]);
-          wv[k][1] = ld_relaxed_u64(src[k] + st);
-          wv[k][2] = ld_relaxed_u64(src[k] + 2 * st);
+#pragma unroll
+          for (int w = 0; w < kRecBase; ++w) wv[k][w] = ld_relaxed_u64(src[k] + w * st);
         }
       }
       if (pub_pending) {
@@ -182,9 +209,12 @@ __device__ void exchange(const PanelArgs& P, unsigned tag, double my_val, int my
       }
 #pragma unroll
       for (int k = 0; k < kMaxPollPerLane; ++k) {
-        if ((pending & (1u << k)) && static_cast<unsigned>(wv[k][0] >> 32) == tag &&
-            static_cast<unsigned>(wv[k][1] >> 32) == tag && static_cast<unsigned>(wv[k][2] >> 32) == tag)
-          pending &= ~(1u << k);
+        if (pending & (1u << k)) {
+          bool all = true;
+#pragma unroll
+          for (int w = 0; w < kRecBase; ++w) all = all && static_cast<unsigned>(wv[k][w] >> 32) == tag;
+          if (all) pending &= ~(1u << k);
+        }
       }
       if (pub_pending && static_cast<unsigned>(pw0 >> 32) == tag && static_cast<unsigned>(pw1 >> 32) == tag)
         pub_pending = false;
@@ -203,15 +233,17 @@ __device__ void exchange(const PanelArgs& P, unsigned tag, double my_val, int my
     }
     fence_acq_rel_gpu();  // acquire what the other CTAs released
     double v = 0.0;
-    int i = INT_MAX;
+    int i = INT_MAX, sl = -1;
     if (ok) {
       for (int k = 0; k < nmine; ++k)
-        argmax_join(v, i, join_hi_lo(wv[k][1], wv[k][2]), static_cast<int>(wv[k][0] & 0xffffffffu));
+        argmax_join(v, i, sl, join_hi_lo(wv[k][1], wv[k][2]), static_cast<int>(wv[k][0] & 0xffffffffu),
+                    static_cast<int>(wv[k][3] & 0xffffffffu));
     }
     for (int off = 16; off > 0; off >>= 1) {
       const double v2 = __shfl_down_sync(0xffffffffu, v, off);
       const int i2 = __shfl_down_sync(0xffffffffu, i, off);
-      argmax_join(v, i, v2, i2);
+      const int s2 = __shfl_down_sync(0xffffffffu, sl, off);
+      argmax_join(v, i, sl, v2, i2, s2);
     }
     const int all_ok = __all_sync(0xffffffffu, ok);
     if (P.pub_ts && blockIdx.x == 0 && all_ok) {
@@ -220,9 +252,9 @@ __device__ void exchange(const PanelArgs& P, unsigned tag, double my_val, int my
       unsigned long long last = 0;
       int who = 0;
       for (int sidx = lane; sidx < P.nslots; sidx += 32) {
-        const unsigned long long v = __ldcg(P.pub_ts + sidx);
-        if (v > last) {
-          last = v;
+        const unsigned long long lv = __ldcg(P.pub_ts + sidx);
+        if (lv > last) {
+          last = lv;
           who = sidx;
         }
       }
@@ -245,6 +277,7 @@ __device__ void exchange(const PanelArgs& P, unsigned tag, double my_val, int my
     if (lane == 0) {
       out->val = v;
       out->idx = i;
+      out->slot = sl;
       out->ok = all_ok;
     }
   }
@@ -282,6 +315,7 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
   extern __shared__ double dsm[];
   __shared__ double s_red_v[kWarps];
   __shared__ int s_red_i[kWarps];
+  __shared__ int s_red_s[kWarps];
   __shared__ double s_pub[kMaxPub];
   __shared__ ExchangeOut s_x;
 
@@ -291,27 +325,30 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
   const int t = threadIdx.x;
   const int n = P.n;
   const int kstart = ldcg(&P.st->kstart[P.panel & 1]);
-  const int S = (n - kstart + G - 1) / G;  // columns per CTA
+  const int S = (n - kstart + G - 1) / G;  // slots per CTA
   const int lo = kstart + c * S;
   const int hi = min(n, lo + S);
+  const int width = max(0, hi - lo);
+  const int nwin = min(P.win_rows, n - kstart);  // panel rows staged per slot
   const long long lda = P.lda, ldw = P.ldw;
   const int ldu = P.ldu;
-  auto owner = [&](int j) -> int { return (j - kstart) / S; };
-  // shared memory: coefficient column, then (when it fits) this CTA's slice
-  // of the panel's workspace rows, wsm[q*S + (j - lo)] = W[q, j].
-  // Stores other CTAs do not need right away stay out of global memory: the
-  // slice of W (flushed at the end of the panel) and the candidate column.
+  auto owner = [&](int z) -> int { return (z - kstart) / S; };
+  // shared memory: coefficient column, candidate column of this CTA's slots,
+  // (when it fits) the slots' panel rows wsm[m*S + (z - lo)], then the maps
   double* coef = dsm;
-  double* wcs = dsm + P.coef_cap;  // candidate values of this CTA's columns
-  double* wsm = (P.w_smem && S <= P.smem_cols) ? wcs + P.smem_cols : nullptr;
-  auto wget = [&](int q, int j) -> double {
-    return wsm ? wsm[q * S + (j - lo)] : ldcg(P.w + q * ldw + j);
+  double* wcs = dsm + P.coef_cap;
+  double* wsm = P.w_smem ? wcs + P.smem_cols : nullptr;
+  int* win = reinterpret_cast<int*>(
+      wcs + P.smem_cols + (P.w_smem ? static_cast<size_t>(P.win_rows) * P.smem_cols : 0));
+  int* mypos = win + P.win_pad;  // index held by slot lo + zz
+  auto wat = [&](int m, int z) -> double& {
+    return wsm ? wsm[m * S + (z - lo)] : P.wslot[m * ldw + z];
   };
-  auto wput = [&](int q, int j, double v) {
-    if (wsm)
-      wsm[q * S + (j - lo)] = v;
-    else
-      P.w[q * ldw + j] = v;
+  // A(x, z) of the symmetric matrix from its upper triangle (A is not written
+  // while the panel runs)
+  auto asym = [&](int x, int z) -> double {
+    return x <= z ? __ldg(P.a + static_cast<long long>(x) * lda + z)
+                  : __ldg(P.a + static_cast<long long>(z) * lda + x);
   };
   const bool timing = P.stats != nullptr && t == 0;
   unsigned long long tm[6] = {0, 0, 0, 0, 0, 0};
@@ -324,65 +361,56 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
     }
   };
 
+  for (int m = t; m < nwin; m += kThreads) win[m] = kstart + m;
+  for (int zz = t; zz < width; zz += kThreads) mypos[zz] = lo + zz;
+  // stage the panel rows of A for this CTA's slots
+  for (int idx = t; idx < nwin * width; idx += kThreads) {
+    const int m = idx / width, zz = idx - m * width;
+    const int x = kstart + m, z = lo + zz;
+    const double* src = x <= z ? P.a + static_cast<long long>(x) * lda + z
+                               : P.a + static_cast<long long>(z) * lda + x;
+    if (wsm)
+      cp_async_8(&wsm[m * S + zz], src);
+    else
+      P.wslot[m * ldw + z] = __ldg(src);
+  }
+  cp_async_wait_all();
+  __syncthreads();
+
   unsigned tag = P.tag_base;
   int p = kstart;
-  // coefficients U[q, p] of the current row: rows q < n_old from Ucm column
-  // coef_src, then lp - n_old (<= 2) values computed by every CTA.
-  int coef_src = p, n_old = 0;
+  // coefficients U[q, p] of the current row: rows q < n_old from the Uslot
+  // column of p's slot, then lp - n_old (<= 2) values computed by every CTA.
+  int n_old = 0;
   double extra0 = 0.0, extra1 = 0.0;
-  int fix_col = -1;          // A[p][fix_col] must be read from fix_src
-  long long fix_src = 0;
   int ncand = 0;
-
-  // Next-row prefetch: the row update of pivot p issues the loads of row p+1
-  // (each thread keeps its own columns, j = lo + t + k*kThreads), so their
-  // HBM latency hides behind the rest of the step.  A prefetched entry can
-  // be stale only in a column that an interchange rewrote meanwhile: the
-  // last step's swap column (fix_col, read from the frozen row instead) and
-  // the swap column of the step before it (prev_swap, re-read once its
-  // write is visible).
-  double nav[kCols];
-  int nav_row = -1;
-  // the next row's coefficient column (rows q < n_old), loaded during the
-  // interchange phase when it has at most 2 * kThreads rows
+  // the next row's coefficient column, loaded during the scaling phase when
+  // it has at most 2 * kThreads rows
   double cpre[2] = {0.0, 0.0};
   bool coef_pre = false;
-  int prev_swap = -1, last_swap = -1;
 
   while (p < P.nominal_end) {
     const int lp = p - kstart;
+    const int sp = win[lp];
+    // the row of p is staged in shared memory unless an interchange gave p a
+    // slot whose staged row was already consumed
+    const bool staged = (sp - kstart) == lp;
     // ---- row update: W[p, j] = A[p, j] - sum_q U[q, p] W[q, j]
     // (CopyCurrentRowToWorkspace + UpdateCurrentRowInWorkspace, :122-162)
     double av[kCols];
-    const bool use_nav = nav_row == p;
 #pragma unroll
     for (int k = 0; k < kCols; ++k) {
-      const int j = lo + t + k * kThreads;
+      const int z = lo + t + k * kThreads;
       double v = 0.0;
-      if (j < hi && j >= p) {
-        if (j == fix_col)
-          v = ldcg(P.a + fix_src);
-        else if (use_nav && j != prev_swap)
-          v = nav[k];
-        else
-          v = ldcg(P.a + p * lda + j);
-      }
+      if (z < hi && mypos[z - lo] >= p) v = staged ? wat(lp, z) : asym(sp, z);
       av[k] = v;
     }
-#pragma unroll
-    for (int k = 0; k < kCols; ++k) {
-      const int j = lo + t + k * kThreads;
-      nav[k] = (j < hi && j > p) ? ldcg(P.a + (p + 1) * lda + j) : 0.0;
-    }
-    nav_row = p + 1;
-    prev_swap = last_swap;
-    last_swap = -1;
     {
-      const double* ucol = P.ucm + static_cast<size_t>(coef_src) * ldu;
       if (coef_pre) {
         if (t < n_old) coef[t] = cpre[0];
         if (t + kThreads < n_old) coef[t + kThreads] = cpre[1];
       } else {
+        const double* ucol = P.uslot + static_cast<size_t>(sp) * ldu;
         for (int q = t; q < n_old; q += kThreads) coef[q] = ldcg(ucol + q);
       }
       if (t == 0) {
@@ -393,37 +421,41 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
     }
     __syncthreads();
     double best = 0.0;
-    int best_j = INT_MAX;
+    int best_j = INT_MAX, best_z = -1;
 #pragma unroll
     for (int k = 0; k < kCols; ++k) {
-      const int j = lo + t + k * kThreads;
-      if (j < hi && j >= p) {
-        const double acc = ordered_dot(coef, lp, [&](int q) { return wget(q, j); });
-        const double wv = xsub(av[k], acc);
-        wput(lp, j, wv);
-        if (j > p) {
-          const double v = fabs(wv);
-          if (v > best) {  // FindCurrentRowMax, :164-182
-            best = v;
-            best_j = j;
+      const int z = lo + t + k * kThreads;
+      if (z < hi) {
+        const int j = mypos[z - lo];
+        if (j >= p) {
+          const double acc = ordered_dot(coef, lp, [&](int q) { return wat(q, z); });
+          const double wv = xsub(av[k], acc);
+          wat(lp, z) = wv;
+          if (j > p) {
+            const double v = fabs(wv);
+            if (v > best || (v == best && j < best_j)) {  // FindCurrentRowMax, :164-182
+              best = v;
+              best_j = j;
+              best_z = z;
+            }
+          } else {
+            s_pub[0] = wv;  // W[p, p]
           }
-        } else {
-          s_pub[0] = wv;  // W[p, p]
+          if (j == p + 1) s_pub[1] = wv;
+          if (j == p + 2) s_pub[2] = wv;
         }
-        if (j == p + 1) s_pub[1] = wv;
-        if (j == p + 2) s_pub[2] = wv;
       }
     }
-    fix_col = -1;
     lap(0);
     int owners[kMaxPub];
-    owners[0] = owner(p);
-    owners[1] = p + 1 < n ? owner(p + 1) : 0;
-    owners[2] = p + 2 < n ? owner(p + 2) : 0;
-    exchange(P, tag++, best, best_j, s_pub, owners, 3, s_red_v, s_red_i, &s_x);
+    owners[0] = owner(sp);
+    owners[1] = lp + 1 < nwin ? owner(win[lp + 1]) : 0;
+    owners[2] = lp + 2 < nwin ? owner(win[lp + 2]) : 0;
+    exchange(P, tag++, best, best_j, best_z, s_pub, owners, 3, s_red_v, s_red_i, s_red_s, &s_x);
     if (!s_x.ok) return;
     const double omega = s_x.val;
     const int r = s_x.idx;
+    const int rs = s_x.slot;  // slot of r
     const double dpp = s_x.pub[0];
     const double w_p1 = s_x.pub[1];  // W[p, p+1] (current-row version)
     const double w_p2 = s_x.pub[2];  // W[p, p+2]
@@ -442,11 +474,11 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
       double cv[kCols];
 #pragma unroll
       for (int k = 0; k < kCols; ++k) {
-        const int i = lo + t + k * kThreads;
-        cv[k] = (i < hi && i >= p) ? (i <= r ? ldcg(P.a + i * lda + r) : ldcg(P.a + r * lda + i)) : 0.0;
+        const int z = lo + t + k * kThreads;
+        cv[k] = (z < hi && mypos[z - lo] >= p) ? asym(z, rs) : 0.0;
       }
       {
-        const double* ucol = P.ucm + static_cast<size_t>(r) * ldu;
+        const double* ucol = P.uslot + static_cast<size_t>(rs) * ldu;
         for (int q = t; q < lp; q += kThreads) coef[q] = ldcg(ucol + q);
         if (t < kMaxPub) s_pub[t] = 0.0;
       }
@@ -454,34 +486,31 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
       double sig = 0.0;
 #pragma unroll
       for (int k = 0; k < kCols; ++k) {
-        const int i = lo + t + k * kThreads;
-        if (i < hi && i >= p) {
-          const double acc = ordered_dot(coef, lp, [&](int q) { return wget(q, i); });
-          const double v = xsub(cv[k], acc);
-          wcs[i - lo] = v;
-          if (i != r) {
-            const double av2 = fabs(v);
-            sig = (sig < av2) ? av2 : sig;  // std::max, FindCandidateColumnMax :354-367
-          } else {
-            s_pub[0] = v;
+        const int z = lo + t + k * kThreads;
+        if (z < hi) {
+          const int i = mypos[z - lo];
+          if (i >= p) {
+            const double acc = ordered_dot(coef, lp, [&](int q) { return wat(q, z); });
+            const double v = xsub(cv[k], acc);
+            wcs[z - lo] = v;
+            if (i != r) {
+              const double av2 = fabs(v);
+              sig = (sig < av2) ? av2 : sig;  // std::max, FindCandidateColumnMax :354-367
+            } else {
+              s_pub[0] = v;
+            }
+            if (i == p) s_pub[1] = v;
+            if (i == p + 1) s_pub[2] = v;
+            if (i == p + 2) s_pub[3] = v;
           }
-          if (i == p) s_pub[1] = v;
-          if (i == p + 1) s_pub[2] = v;
-          if (i == p + 2) s_pub[3] = v;
         }
       }
-      // stage W[q, p] and W[q, p+1] (q < lp) for the owner of r: the
-      // interchange moves one of these columns into column r
-      if (p >= lo && p < hi)
-        for (int q = t; q < lp; q += kThreads) P.wstage[q] = wget(q, p);
-      if (p + 1 >= lo && p + 1 < hi)
-        for (int q = t; q < lp; q += kThreads) P.wstage[P.coef_cap + q] = wget(q, p + 1);
       lap(2);
-      owners[0] = owner(r);
-      owners[1] = owner(p);
-      owners[2] = p + 1 < n ? owner(p + 1) : 0;
-      owners[3] = p + 2 < n ? owner(p + 2) : 0;
-      exchange(P, tag++, sig, 0, s_pub, owners, 4, s_red_v, s_red_i, &s_x);
+      owners[0] = owner(rs);
+      owners[1] = owner(sp);
+      owners[2] = lp + 1 < nwin ? owner(win[lp + 1]) : 0;
+      owners[3] = lp + 2 < nwin ? owner(win[lp + 2]) : 0;
+      exchange(P, tag++, sig, 0, 0, s_pub, owners, 4, s_red_v, s_red_i, s_red_s, &s_x);
       if (!s_x.ok) return;
       const double sigma = s_x.val;
       wc_r = s_x.pub[0];
@@ -508,172 +537,106 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
       // reference's W(p, r) holds the column version of that entry.
       const double d = dpp;
       const double den = safe_denominator(d);
-      for (int j = max(lo, p + 1) + t; j < hi; j += kThreads) {
-        double wv;
-        if (cand && j == r) {
-          wv = wc_p;
-          wput(lp, j, wv);
-        } else {
-          wv = wget(lp, j);
+#pragma unroll
+      for (int k = 0; k < kCols; ++k) {
+        const int z = lo + t + k * kThreads;
+        if (z < hi) {
+          const int j = mypos[z - lo];
+          if (j > p) {
+            double wv;
+            if (cand && j == r) {
+              wv = wc_p;
+              wat(lp, z) = wv;
+            } else {
+              wv = wat(lp, z);
+            }
+            P.uslot[static_cast<size_t>(z) * ldu + lp] = div_or_zero(wv, den);
+          }
         }
-        P.ucm[static_cast<size_t>(j) * ldu + lp] = div_or_zero(wv, den);
       }
-      if (c == owner(p)) {
-        for (int q = t; q < lp; q += kThreads)
-          P.uout[static_cast<size_t>(lp) * ldu + q] = ldcg(P.ucm + static_cast<size_t>(p) * ldu + q);
-        if (t == 0) {
-          P.uout[static_cast<size_t>(lp) * ldu + lp] = d;
-          P.ptype[p] = 1;
-        }
+      if (c == 0 && t == 0) {
+        P.dlog[2 * lp] = d;
+        P.ptype[p] = 1;
       }
       // next row's coefficients: U[q, p+1] for q < p, then U[p, p+1]
-      coef_src = p + 1;
       n_old = lp;
       extra0 = div_or_zero((cand && r == p + 1) ? wc_p : w_p1, den);
       p += 1;
     } else if (kind == -1) {
-      // SwapOneByOnePivot (:392-401, :414-498) + ScaleOneByOnePivot.
+      // SwapOneByOnePivot (:392-401, :414-498) + ScaleOneByOnePivot: p and r
+      // exchange slots; the new row p is the candidate column.
       const double d = wc_r;
       const double den = safe_denominator(d);
-      for (int j = max(lo, p) + t; j < hi; j += kThreads) {
-        if (j == p) {
-          wput(lp, j, d);
-          continue;
-        }
-        const double wv = (j == r) ? wc_p : wcs[j - lo];
-        wput(lp, j, wv);
-        P.ucm[static_cast<size_t>(j) * ldu + lp] = div_or_zero(wv, den);
-        // old row p moves to row r (j > r) / column r (j < r); row p itself
-        // stays frozen so other CTAs may still read it.
-        const double old_apj = ldcg(P.a + p * lda + j);
-        if (j > r) {
-          P.a[r * lda + j] = old_apj;
-        } else if (j < r) {
-          P.a[j * lda + r] = old_apj;
-        } else {
-          P.a[r * lda + r] = ldcg(P.a + p * lda + p);
-        }
+      if (t == 0) {
+        win[lp] = rs;
+        if (r - kstart < nwin) win[r - kstart] = sp;
+        if (sp >= lo && sp < hi) mypos[sp - lo] = r;
+        if (rs >= lo && rs < hi) mypos[rs - lo] = p;
       }
-      if (c == owner(r)) {
-        for (int q = t; q < lp; q += kThreads) {
-          const double ur = ldcg(P.ucm + static_cast<size_t>(r) * ldu + q);
-          P.uout[static_cast<size_t>(lp) * ldu + q] = ur;  // final column p
-          P.ucm[static_cast<size_t>(r) * ldu + q] = ldcg(P.ucm + static_cast<size_t>(p) * ldu + q);
-          wput(q, r, ldcg(P.wstage + q));
+      __syncthreads();
+#pragma unroll
+      for (int k = 0; k < kCols; ++k) {
+        const int z = lo + t + k * kThreads;
+        if (z < hi && mypos[z - lo] > p) {
+          const double wv = wcs[z - lo];
+          wat(lp, z) = wv;
+          P.uslot[static_cast<size_t>(z) * ldu + lp] = div_or_zero(wv, den);
         }
-      }
-      // previously factored rows: columns p and r exchange (:472-491)
-      for (int i = c * kThreads + t; i < kstart; i += G * kThreads) {
-        double* x = P.a + i * lda + p;
-        double* y = P.a + i * lda + r;
-        const double tx = *x;
-        *x = *y;
-        *y = tx;
       }
       if (c == 0 && t == 0) {
-        P.uout[static_cast<size_t>(lp) * ldu + lp] = d;
+        P.dlog[2 * lp] = d;
         P.ptype[p] = 1;
-        const int tp = P.perm[p];
-        P.perm[p] = P.perm[r];
-        P.perm[r] = tp;
       }
-      coef_src = (r == p + 1) ? p : p + 1;
       n_old = lp;
       extra0 = div_or_zero((r == p + 1) ? wc_p : wc_p1, den);
-      if (p + 1 < r) {
-        fix_col = r;
-        fix_src = p * lda + (p + 1);  // new A[p+1, r] = old A[p, p+1]
-      } else {
-        // r == p+1: the next row is the old row p (its diagonal is old A[p, p])
-#pragma unroll
-        for (int k = 0; k < kCols; ++k) {
-          const int j = lo + t + k * kThreads;
-          nav[k] = (j < hi && j > p + 1) ? av[k] : ((j == p + 1 && j < hi) ? ldcg(P.a + p * lda + p) : 0.0);
-        }
-      }
-      last_swap = r;
       p += 1;
     } else {
-      // SwapTwoByTwoPivot (:403-412, :500-587) + ScaleTwoByTwoPivot (:658-704)
-      const int s = p + 1, ls = lp + 1;
+      // SwapTwoByTwoPivot (:403-412, :500-587) + ScaleTwoByTwoPivot (:658-704):
+      // p+1 and r exchange slots; row p+1 is the candidate column.
+      const int ls = lp + 1;
+      const int ss = win[ls];
       const double d11 = dpp, d21 = wc_p, d22 = wc_r;
       const double det = xsub(xmul(d11, d22), xmul(d21, d21));
       const double i11 = xdiv(d22, det);
       const double i22 = xdiv(d11, det);
       const double i21 = xdiv(-d21, det);
-      for (int j = max(lo, p + 2) + t; j < hi; j += kThreads) {
-        double x;
-        if (j == r) {
-          x = w_p1;  // W(p, s) and W(p, r) exchange
-          wput(lp, j, x);
-        } else {
-          x = wget(lp, j);
-        }
-        const double y = (j == r) ? wc_p1 : wcs[j - lo];
-        wput(ls, j, y);
-        P.ucm[static_cast<size_t>(j) * ldu + lp] = xadd(xmul(i11, x), xmul(i21, y));
-        P.ucm[static_cast<size_t>(j) * ldu + ls] = xadd(xmul(i21, x), xmul(i22, y));
-        if (r != s) {
-          const double old_asj = ldcg(P.a + s * lda + j);
-          if (j > r) {
-            P.a[r * lda + j] = old_asj;
-          } else if (j < r) {
-            P.a[j * lda + r] = old_asj;
-          } else {
-            P.a[r * lda + r] = ldcg(P.a + s * lda + s);
-          }
-        }
+      __syncthreads();  // every thread has read win[ls]
+      if (r != p + 1 && t == 0) {
+        win[ls] = rs;
+        if (r - kstart < nwin) win[r - kstart] = ss;
+        if (ss >= lo && ss < hi) mypos[ss - lo] = r;
+        if (rs >= lo && rs < hi) mypos[rs - lo] = p + 1;
       }
-      if (c == owner(p)) {
-        for (int q = t; q < lp; q += kThreads)
-          P.uout[static_cast<size_t>(lp) * ldu + q] = ldcg(P.ucm + static_cast<size_t>(p) * ldu + q);
-      }
-      if (c == owner(r)) {
-        for (int q = t; q < lp; q += kThreads) {
-          const double ur = ldcg(P.ucm + static_cast<size_t>(r) * ldu + q);
-          P.uout[static_cast<size_t>(ls) * ldu + q] = ur;  // final column s
-          if (r != s) {
-            P.ucm[static_cast<size_t>(r) * ldu + q] = ldcg(P.ucm + static_cast<size_t>(s) * ldu + q);
-            wput(q, r, ldcg(P.wstage + P.coef_cap + q));
-          }
-        }
-      }
-      if (r != s) {
-        for (int i = c * kThreads + t; i < kstart; i += G * kThreads) {
-          double* x = P.a + i * lda + s;
-          double* y = P.a + i * lda + r;
-          const double tx = *x;
-          *x = *y;
-          *y = tx;
+      __syncthreads();
+#pragma unroll
+      for (int k = 0; k < kCols; ++k) {
+        const int z = lo + t + k * kThreads;
+        if (z < hi && mypos[z - lo] > p + 1) {
+          const double x = wat(lp, z);
+          const double y = wcs[z - lo];
+          wat(ls, z) = y;
+          P.uslot[static_cast<size_t>(z) * ldu + lp] = xadd(xmul(i11, x), xmul(i21, y));
+          P.uslot[static_cast<size_t>(z) * ldu + ls] = xadd(xmul(i21, x), xmul(i22, y));
         }
       }
       if (c == 0 && t == 0) {
-        P.uout[static_cast<size_t>(lp) * ldu + lp] = d11;
-        P.uout[static_cast<size_t>(ls) * ldu + lp] = d21;
-        P.uout[static_cast<size_t>(ls) * ldu + ls] = d22;
+        P.dlog[2 * lp] = d11;
+        P.dlog[2 * lp + 1] = d21;
+        P.dlog[2 * ls] = d22;
         P.ptype[p] = 2;
-        P.ptype[s] = -2;
-        const int tp = P.perm[s];
-        P.perm[s] = P.perm[r];
-        P.perm[r] = tp;
+        P.ptype[p + 1] = -2;
       }
-      // next row p+2: coefficients U[q, p+2], q < p, then U[p, p+2], U[s, p+2]
+      // next row p+2: coefficients U[q, p+2], q < p, then U[p, p+2], U[p+1, p+2]
       const double x = (r == p + 2) ? w_p1 : w_p2;
       const double y = (r == p + 2) ? wc_p1 : wc_p2;
-      coef_src = (r == p + 2) ? s : p + 2;
       n_old = lp;
       extra0 = xadd(xmul(i11, x), xmul(i21, y));
       extra1 = xadd(xmul(i21, x), xmul(i22, y));
-      if (p + 2 < r) {
-        fix_col = r;
-        fix_src = s * lda + (p + 2);  // new A[p+2, r] = old A[s, p+2]
-      }
-      if (r != s) last_swap = r;
       p += 2;
     }
-    coef_pre = n_old <= 2 * kThreads;
+    coef_pre = n_old <= 2 * kThreads && p < P.nominal_end;
     if (coef_pre) {
-      const double* ucol = P.ucm + static_cast<size_t>(coef_src) * ldu;
+      const double* ucol = P.uslot + static_cast<size_t>(win[p - kstart]) * ldu;
       cpre[0] = t < n_old ? ldcg(ucol + t) : 0.0;
       cpre[1] = t + kThreads < n_old ? ldcg(ucol + t + kThreads) : 0.0;
     }
@@ -683,37 +646,130 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
 
   if (P.stats && t == 0)
     for (int k = 0; k < 5; ++k) atomicAdd(P.stats + 16 + 2048 + c * 5 + k, tm[k]);
-  // the trailing update reads W from global memory
-  if (wsm) {
-    const int kb = p - kstart;
-    for (int q = 0; q < kb; ++q)
-      for (int j = lo + t; j < hi; j += kThreads) P.w[q * ldw + j] = wsm[q * S + (j - lo)];
+  const int e = p;
+  const int kb = e - kstart;
+  // ---- the panel's W and U in final column order, the slot of every index,
+  // and the list of indices whose slot changed
+  __syncthreads();
+  for (int idx = t; idx < width * kb; idx += kThreads) {
+    const int zz = idx / kb, q = idx - zz * kb;
+    P.ucm[static_cast<size_t>(mypos[zz]) * ldu + q] = P.uslot[static_cast<size_t>(lo + zz) * ldu + q];
+  }
+  for (int idx = t; idx < width * kb; idx += kThreads) {
+    const int q = idx / width, zz = idx - q * width;
+    const int x = mypos[zz];
+    if (x >= e) P.w[q * ldw + x] = wat(q, lo + zz);
+  }
+  for (int zz = t; zz < width; zz += kThreads) {
+    const int x = mypos[zz], z = lo + zz;
+    P.srcmap[x] = z;
+    if (x != z) {
+      const int slot_i = atomicAdd(&P.st->moved[P.panel & 1], 1);
+      P.moved[(P.panel & 1) * P.move_cap + slot_i] = x;
+    }
   }
   if (c == 0 && t == 0) {
-    // panel range [kstart, p); the next panel starts at p.
-    P.st->kstart[(P.panel + 1) & 1] = p;
-    if (P.panel_end) P.panel_end[P.panel] = p;
+    // panel range [kstart, e); the next panel starts at e.
+    P.st->kstart[(P.panel + 1) & 1] = e;
+    if (P.panel_end) P.panel_end[P.panel] = e;
     if (P.stats) {
       for (int k = 0; k < 5; ++k) atomicAdd(P.stats + k, tm[k]);
-      atomicAdd(P.stats + 5, static_cast<unsigned long long>(p - kstart));
+      atomicAdd(P.stats + 5, static_cast<unsigned long long>(kb));
       atomicAdd(P.stats + 6, static_cast<unsigned long long>(ncand));
     }
   }
+  // grid barrier: every CTA's maps and lists are visible after it
+  {
+    int owners0[kMaxPub] = {0, 0, 0, 0, 0, 0};
+    exchange(P, tag++, 0.0, 0, 0, s_pub, owners0, 0, s_red_v, s_red_i, s_red_s, &s_x);
+    if (!s_x.ok) return;
+  }
+  // ---- gather the interchanged data (written back by finalize_kernel)
+  const int cnt = ldcg(&P.st->moved[P.panel & 1]);
+  if (cnt == 0) return;
+  const int* list = P.moved + (P.panel & 1) * P.move_cap;
+  const long long m = n - kstart;
+  const long long nthreads = static_cast<long long>(G) * kThreads;
+  const long long gtid = static_cast<long long>(c) * kThreads + t;
+  // rows of the moved indices over the active columns: gbuf[ix][y - k0] = A(src x, src y)
+  for (long long idx = gtid; idx < cnt * m; idx += nthreads) {
+    const int ix = static_cast<int>(idx / m);
+    const int y = kstart + static_cast<int>(idx - ix * m);
+    const int sx = ldcg(P.srcmap + ldcg(list + ix));
+    const int sy = ldcg(P.srcmap + y);
+    P.gbuf[ix * ldw + (y - kstart)] = asym(sx, sy);
+  }
+  // factored rows q < k0 at the moved columns (their column exchanges, :472-491)
+  for (long long idx = gtid; idx < static_cast<long long>(kstart) * cnt; idx += nthreads) {
+    const int q = static_cast<int>(idx / cnt), ix = static_cast<int>(idx - static_cast<long long>(q) * cnt);
+    const int sx = ldcg(P.srcmap + ldcg(list + ix));
+    P.gbuf2[static_cast<long long>(q) * P.move_cap + ix] = __ldg(P.a + static_cast<long long>(q) * lda + sx);
+  }
+  for (long long ix = gtid; ix < cnt; ix += nthreads)
+    P.permbuf[ix] = ldcg(P.perm + ldcg(P.srcmap + ldcg(list + ix)));
 }
 
-// Writes the panel's compact factor rows [k0, e) into A:
-// A[q, j] = Uout (pivot columns j < e) or Ucm (trailing columns j >= e).
+// Writes back what the panel's interchanges moved, the permutation, and the
+// panel's compact factor rows [k0, e):
+//   A[x, y]  (moved x >= e, y >= e)        from the gathered rows
+//   A[q, x]  (q < k0, moved x)             from the gathered factored rows
+//   perm[x]  (moved x)                     = perm[slot of x] before the panel
+//   A[q, j]  (k0 <= q < e, j >= q)         D entries (dlog) or U[q, j] (ucm)
+struct FinArgs {
+  double* a;
+  long long lda;
+  const double* ucm;
+  int ldu;
+  const double* dlog;
+  const int* ptype;
+  const int* moved;
+  int move_cap;
+  const double* gbuf;
+  long long ldg;
+  const double* gbuf2;
+  const int* permbuf;
+  int* perm;
+  int n;
+  DeviceState* st;
+  int panel;
+};
+
 constexpr int kFinTile = 32;
-__global__ void __launch_bounds__(256) finalize_kernel(double* a, long long lda, const double* ucm,
-                                                       int ldu, const double* uout, int n,
-                                                       DeviceState* st, int panel) {
+__global__ void __launch_bounds__(256) finalize_kernel(FinArgs F) {
   __shared__ double tile[kFinTile][kFinTile + 1];
-  if (ld_relaxed_s32(&st->abort)) return;
-  const int k0 = ldcg(&st->kstart[panel & 1]);
-  const int e = ldcg(&st->kstart[(panel + 1) & 1]);
+  if (ld_relaxed_s32(&F.st->abort)) return;
+  const int k0 = ldcg(&F.st->kstart[F.panel & 1]);
+  const int e = ldcg(&F.st->kstart[(F.panel + 1) & 1]);
   const int kb = e - k0;
+  const int n = F.n;
+  const long long lda = F.lda;
+  const long long nthreads = static_cast<long long>(gridDim.x) * blockDim.x;
+  const long long gtid = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  // the next panel counts its moved indices from zero
+  if (gtid == 0) F.st->moved[(F.panel + 1) & 1] = 0;
+  const int cnt = ldcg(&F.st->moved[F.panel & 1]);
+  const int* list = F.moved + (F.panel & 1) * F.move_cap;
+  if (cnt > 0) {
+    const long long m = n - e;
+    for (long long idx = gtid; idx < cnt * m; idx += nthreads) {
+      const int ix = static_cast<int>(idx / m);
+      const int x = list[ix];
+      if (x < e) continue;
+      const int y = e + static_cast<int>(idx - ix * m);
+      const double v = F.gbuf[ix * F.ldg + (y - k0)];
+      if (x <= y)
+        F.a[static_cast<long long>(x) * lda + y] = v;
+      else
+        F.a[static_cast<long long>(y) * lda + x] = v;
+    }
+    for (long long idx = gtid; idx < static_cast<long long>(k0) * cnt; idx += nthreads) {
+      const int q = static_cast<int>(idx / cnt), ix = static_cast<int>(idx - static_cast<long long>(q) * cnt);
+      F.a[static_cast<long long>(q) * lda + list[ix]] = F.gbuf2[static_cast<long long>(q) * F.move_cap + ix];
+    }
+    for (long long ix = gtid; ix < cnt; ix += nthreads) F.perm[list[ix]] = F.permbuf[ix];
+  }
   if (kb <= 0) return;
-  // tiles over (q in [0, kb), j in [k0, n))
+  // compact rows: tiles over (q in [0, kb), j in [k0, n))
   const int qt = (kb + kFinTile - 1) / kFinTile;
   const int jt = (n - k0 + kFinTile - 1) / kFinTile;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
@@ -724,16 +780,21 @@ __global__ void __launch_bounds__(256) finalize_kernel(double* a, long long lda,
     for (int jj = ty; jj < kFinTile; jj += 8) {
       const int j = j0 + jj, q = q0 + tx;
       double v = 0.0;
-      if (j < n && q < kb) {
-        v = (j < e) ? uout[static_cast<size_t>(j - k0) * ldu + q]
-                    : ucm[static_cast<size_t>(j) * ldu + q];
+      if (j < n && q < kb && j >= k0 + q) {
+        const int lj = j - k0;
+        if (j < e && q == lj)
+          v = F.dlog[2 * lj];  // D(l, l)
+        else if (j < e && q == lj - 1 && F.ptype[j] == -2)
+          v = F.dlog[2 * q + 1];  // D(l, l+1) of a 2x2
+        else
+          v = F.ucm[static_cast<size_t>(j) * F.ldu + q];
       }
       tile[jj][tx] = v;
     }
     __syncthreads();
     for (int qq = ty; qq < kFinTile; qq += 8) {
       const int q = q0 + qq, j = j0 + tx;
-      if (q < kb && j < n && j >= k0 + q) a[static_cast<size_t>(k0 + q) * lda + j] = tile[tx][qq];
+      if (q < kb && j < n && j >= k0 + q) F.a[static_cast<size_t>(k0 + q) * lda + j] = tile[tx][qq];
     }
     __syncthreads();
   }
@@ -753,6 +814,8 @@ __global__ void init_kernel(int n, int* perm, int* pivot_types, DeviceState* st,
     st->kstart[1] = 0;
     st->abort = 0;
     st->status = 0;
+    st->moved[0] = 0;
+    st->moved[1] = 0;
   }
 }
 
@@ -768,6 +831,7 @@ __global__ void status_copy_kernel(const DeviceState* st, int* out) {
 __global__ void __launch_bounds__(kThreads) probe_kernel(PanelArgs P) {
   __shared__ double s_red_v[kWarps];
   __shared__ int s_red_i[kWarps];
+  __shared__ int s_red_s[kWarps];
   __shared__ double s_pub[kMaxPub];
   __shared__ ExchangeOut s_x;
   if (threadIdx.x < kMaxPub) s_pub[threadIdx.x] = 0.0;
@@ -775,8 +839,8 @@ __global__ void __launch_bounds__(kThreads) probe_kernel(PanelArgs P) {
   __syncthreads();
   const unsigned long long t0 = globaltimer_ns();
   for (int it = 0; it < P.n; ++it) {
-    exchange(P, P.tag_base + it, static_cast<double>(blockIdx.x), blockIdx.x, s_pub, owners, 3,
-             s_red_v, s_red_i, &s_x);
+    exchange(P, P.tag_base + it, static_cast<double>(blockIdx.x), blockIdx.x, blockIdx.x, s_pub, owners,
+             3, s_red_v, s_red_i, s_red_s, &s_x);
     if (!s_x.ok) return;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0 && P.stats) P.stats[0] = globaltimer_ns() - t0;
@@ -827,15 +891,23 @@ int launch_panel(const FactorPlan& plan, int panel, cudaStream_t s) {
   const long long nominal = static_cast<long long>(panel + 1) * plan.b;
   P.nominal_end = nominal < plan.n ? static_cast<int>(nominal) : plan.n;
   P.can_shift = panel + 1 < plan.nb;
+  P.win_rows = plan.b + 2;
+  P.win_pad = static_cast<int>(align_up(static_cast<size_t>(plan.b) + 2, 2));
   P.a = plan.a;
   P.lda = plan.lda;
   P.w = plan.w;
   P.ldw = plan.ldw;
+  P.wslot = plan.wslot;
+  P.uslot = plan.uslot;
   P.ucm = plan.ucm;
   P.ldu = plan.ldu;
-  P.uout = plan.uout;
-  P.wc = plan.wc;
-  P.wstage = plan.wc + align_up(static_cast<size_t>(plan.n), 64);
+  P.dlog = plan.dlog;
+  P.srcmap = plan.srcmap;
+  P.moved = plan.moved;
+  P.move_cap = plan.move_cap;
+  P.gbuf = plan.gbuf;
+  P.gbuf2 = plan.gbuf2;
+  P.permbuf = plan.permbuf;
   P.perm = plan.perm;
   P.ptype = plan.pivot_types;
   P.panel_end = plan.panel_end;
@@ -855,15 +927,17 @@ int launch_panel(const FactorPlan& plan, int panel, cudaStream_t s) {
   P.poll_ns = poll_ns;
   if (plan.grid > 32 * kMaxPollPerLane)
     return set_error(BBK_ERR_INVALID_ARGUMENT, "panel grid %d exceeds %d", plan.grid, 32 * kMaxPollPerLane);
-  // shared memory: coefficient column + (if it fits) the CTA's W slice
+  // shared memory: coefficient column + candidate column + (if it fits) the
+  // slots' panel rows, then the window map and the slot -> index map
   const int smax = (plan.n + plan.grid - 1) / plan.grid;
   P.coef_cap = static_cast<int>(align_up(static_cast<size_t>(plan.b) + 4, 2));
-  size_t bytes = (static_cast<size_t>(P.coef_cap) + smax) * sizeof(double);
-  const size_t wbytes = static_cast<size_t>(plan.b + 2) * smax * sizeof(double);
-  const size_t limit = 220 * 1024;
-  P.w_smem = bytes + wbytes <= limit;
   P.smem_cols = smax;
-  if (P.w_smem) bytes += wbytes;
+  const size_t base = (static_cast<size_t>(P.coef_cap) + smax) * sizeof(double) +
+                      (static_cast<size_t>(P.win_pad) + smax) * sizeof(int);
+  const size_t wbytes = static_cast<size_t>(P.win_rows) * smax * sizeof(double);
+  const size_t limit = 220 * 1024;
+  P.w_smem = base + wbytes <= limit;
+  const size_t bytes = base + (P.w_smem ? wbytes : 0);
   BBK_CUDA_TRY(cudaFuncSetAttribute(panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(bytes)));
   void* kargs[] = {&P};
@@ -876,8 +950,24 @@ int launch_panel(const FactorPlan& plan, int panel, cudaStream_t s) {
 
 int launch_finalize(const FactorPlan& plan, int panel, cudaStream_t s) {
   const int sms = device_sm_count();
-  finalize_kernel<<<2 * sms, 256, 0, s>>>(plan.a, plan.lda, plan.ucm, plan.ldu, plan.uout,
-                                          plan.n, plan.state, panel);
+  FinArgs F{};
+  F.a = plan.a;
+  F.lda = plan.lda;
+  F.ucm = plan.ucm;
+  F.ldu = plan.ldu;
+  F.dlog = plan.dlog;
+  F.ptype = plan.pivot_types;
+  F.moved = plan.moved;
+  F.move_cap = plan.move_cap;
+  F.gbuf = plan.gbuf;
+  F.ldg = plan.ldw;
+  F.gbuf2 = plan.gbuf2;
+  F.permbuf = plan.permbuf;
+  F.perm = plan.perm;
+  F.n = plan.n;
+  F.st = plan.state;
+  F.panel = panel;
+  finalize_kernel<<<2 * sms, 256, 0, s>>>(F);
   BBK_CUDA_TRY(cudaGetLastError());
   count_launch();
   return BBK_OK;
