@@ -60,6 +60,14 @@ __device__ __forceinline__ int ld_relaxed_s32(const int* p) {
   asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void red_release_add_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
 __device__ __forceinline__ void fence_acq_rel_gpu() {
   asm volatile("fence.acq_rel.gpu;" ::: "memory");
 }
@@ -76,15 +84,20 @@ struct DeviceState {
   int abort;      // nonzero: a kernel gave up; every later kernel returns
   int status;     // bbk_status of the factorization
   int moved[2];   // panel P: count of indices its interchanges moved, in moved[P & 1]
+  int xseq[2];    // exchanges completed before panel P, in xseq[P & 1]
+  int pad[24];    // the arrival counter gets a cache line of its own
+  unsigned long long xcount;  // arrivals at grid exchanges (one per CTA per exchange)
 };
 
 // ---------------------------------------------------------------------------
-// Tagged-slot exchange: a grid-wide barrier fused with an all-gather of one
-// small record per CTA.  Every 64-bit word carries the exchange's 32-bit tag
-// in its high half, so a reader knows a word is current without any other
-// ordering; the writer's release fence before its stores and the reader's
-// acquire fence after seeing all tags order everything else.  Two slot sets
-// alternate (tag parity): no CTA can be two exchanges ahead of another.
+// Grid exchange: a grid-wide barrier fused with an all-gather of one small
+// record per CTA.  Each CTA stores its record, then adds one to an arrival
+// counter with release semantics; every CTA polls that single word with
+// acquire loads until all CTAs of this exchange have arrived, and only then
+// reads the records (one pass).  Every record word also carries the
+// exchange's 32-bit tag in its high half, which the reader checks.  Two
+// record sets alternate (tag parity): no CTA can be two exchanges ahead of
+// another.
 // ---------------------------------------------------------------------------
 constexpr int kSlotWords = 16;   // words per CTA record
 constexpr int kMaxPub = 6;       // published doubles per record

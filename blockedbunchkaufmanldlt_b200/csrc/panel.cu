@@ -31,8 +31,8 @@
 // permutation, and the panel's compact factor rows.
 //
 // Per pivot step the grid meets once (no candidate) or twice (candidate
-// column needed), in a tagged-record exchange that is also the argmax
-// reduction.
+// column needed), in an exchange (arrival counter + one record per CTA) that
+// is also the argmax reduction.
 #include <climits>
 #include <cstdio>
 #include <cstdlib>
@@ -49,7 +49,7 @@ namespace {
 constexpr int kThreads = BBK_PANEL_THREADS;
 constexpr int kWarps = kThreads / 32;
 constexpr int kCols = 4;  // slots per thread: S <= kCols * kThreads
-constexpr int kMaxPollPerLane = 8;  // exchange records polled per lane (grid <= 256)
+constexpr int kMaxGrid = 256;  // CTAs of a panel launch (records per exchange)
 constexpr int kRecBase = 4;  // record words before the published doubles: idx, hi, lo, slot
 static_assert(kRecBase + 2 * kMaxPub <= kSlotWords, "record too large");
 
@@ -82,14 +82,13 @@ struct PanelArgs {
   DeviceState* st;
   int nslots;        // records each exchange waits for (gridDim.x normally)
   int slot_stride;   // records per parity in `slots` (>= nslots)
-  unsigned tag_base;
   unsigned long long timeout_ns;
   int coef_cap;      // doubles reserved for the coefficient column
   int w_smem;        // keep this CTA's panel rows in shared memory
   int smem_cols;     // slice width the shared-memory allocation holds
   unsigned long long* stats;  // optional per-phase nanoseconds (CTA 0)
   unsigned long long* pub_ts; // with stats: each CTA's publish timestamp
-  unsigned poll_ns;           // pause between polls of the exchange records
+  unsigned poll_ns;           // pause between polls of the arrival counter
 };
 
 struct ExchangeOut {
@@ -129,12 +128,13 @@ __device__ __forceinline__ void cp_async_8(double* smem_dst, const double* gsrc)
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // CTA-collective: reduce (my_val, my_idx, my_slot) over the CTA, publish the
-// CTA's record (reduction + its kMaxPub scalars in pub_in), wait for the
-// records of all `nslots` CTAs, and return the grid-wide argmax plus pub[k]
-// taken from the record of CTA pub_owner[k].  Must be called by every thread.
-__device__ void exchange(const PanelArgs& P, unsigned tag, double my_val, int my_idx, int my_slot,
-                         const double* pub_in, const int* pub_owner, int npub, double* s_red_v,
-                         int* s_red_i, int* s_red_s, ExchangeOut* out) {
+// CTA's record (reduction + its kMaxPub scalars in pub_in), wait until the
+// arrival counter reaches `target` (all `nslots` CTAs of this exchange), and
+// return the grid-wide argmax plus pub[k] taken from the record of CTA
+// pub_owner[k].  Must be called by every thread.
+__device__ void exchange(const PanelArgs& P, unsigned tag, unsigned long long target, double my_val,
+                         int my_idx, int my_slot, const double* pub_in, const int* pub_owner,
+                         int npub, double* s_red_v, int* s_red_i, int* s_red_s, ExchangeOut* out) {
   const int t = threadIdx.x;
   const int lane = t & 31, warp = t >> 5;
   for (int off = 16; off > 0; off >>= 1) {
@@ -148,10 +148,10 @@ __device__ void exchange(const PanelArgs& P, unsigned tag, double my_val, int my
     s_red_i[warp] = my_idx;
     s_red_s[warp] = my_slot;
   }
-  __syncthreads();  // also orders this CTA's global writes before the fences
+  __syncthreads();  // also orders this CTA's global writes before the release
   // Structure-of-arrays records: word w of CTA c lives at
   // slots[((tag & 1) * kSlotWords + w) * slot_stride + c], so one warp load
-  // polls word w of 32 consecutive CTAs in two cache lines.
+  // reads word w of 32 consecutive CTAs in two cache lines.
   unsigned long long* par_base =
       P.slots + static_cast<size_t>(tag & 1u) * kSlotWords * P.slot_stride;
   if (warp == 0) {
@@ -171,83 +171,72 @@ __device__ void exchange(const PanelArgs& P, unsigned tag, double my_val, int my
         const bool high = lane < 3 ? lane == 1 : ((lane - kRecBase) & 1) == 0;
         word = high ? static_cast<unsigned>(bits >> 32) : static_cast<unsigned>(bits);
       }
-      if (P.pub_ts && lane == 0) P.pub_ts[blockIdx.x] = globaltimer_ns();
-      fence_acq_rel_gpu();  // release everything this CTA wrote so far
       st_relaxed_u64(par_base + static_cast<size_t>(lane) * P.slot_stride + blockIdx.x,
                      tag_word(tag, word));
     }
-  }
-  if (warp == 0) {
-    // Every lane polls all of its records (CTAs lane, lane+32, ...) and its
-    // published word pair at once, so the exchange completes one L2 round trip
-    // after the last record lands.
-    const size_t st = P.slot_stride;
-    const unsigned long long* src[kMaxPollPerLane];
-    unsigned long long wv[kMaxPollPerLane][kRecBase];
-    int nmine = 0;
-    for (int sidx = lane; sidx < P.nslots && nmine < kMaxPollPerLane; sidx += 32)
-      src[nmine++] = par_base + sidx;
-    const bool has_pub = lane < npub;
-    const unsigned long long* psrc =
-        has_pub ? par_base + static_cast<size_t>(kRecBase + 2 * lane) * st + pub_owner[lane] : par_base;
-    unsigned pending = (1u << nmine) - 1u;
-    bool pub_pending = has_pub;
-    unsigned long long pw0 = 0, pw1 = 0;
+    __syncwarp();
+    if (lane == 0) {
+      if (P.pub_ts) P.pub_ts[blockIdx.x] = globaltimer_ns();
+      // releases this CTA's record and everything the CTA wrote before it
+      red_release_add_u64(&P.st->xcount, 1ull);
+    }
+    // Every lane polls the arrival counter (one request per warp load); the
+    // acquire load orders the record reads after it.
     const unsigned long long t0 = globaltimer_ns();
     bool ok = true;
-    for (unsigned iter = 1; pending || pub_pending; ++iter) {
-#pragma unroll
-      for (int k = 0; k < kMaxPollPerLane; ++k) {
-        if (pending & (1u << k)) {
-#pragma unroll
-          for (int w = 0; w < kRecBase; ++w) wv[k][w] = ld_relaxed_u64(src[k] + w * st);
+    for (unsigned iter = 1;; ++iter) {
+      if (__all_sync(0xffffffffu, ld_acquire_u64(&P.st->xcount) >= target)) break;
+      if (P.poll_ns) __nanosleep(P.poll_ns);
+      if ((iter & 31u) == 0) {
+        const bool stop = ld_relaxed_s32(&P.st->abort) != 0;
+        const bool late = globaltimer_ns() - t0 > P.timeout_ns;
+        if (__any_sync(0xffffffffu, stop || late)) {
+          if (lane == 0 && !stop) fail(P.st, BBK_ERR_TIMEOUT);
+          ok = false;
+          break;
         }
       }
-      if (pub_pending) {
+    }
+    // one pass over the records (CTAs lane, lane+32, ...) and this lane's
+    // published word pair; the tags confirm every word is this exchange's
+    const size_t st = P.slot_stride;
+    double v2 = 0.0;
+    int i2 = INT_MAX, s2 = -1;
+    unsigned long long pw0 = 0, pw1 = 0;
+    const bool has_pub = lane < npub;
+    if (ok) {
+      bool tags_ok = true;
+      for (int sidx = lane; sidx < P.nslots; sidx += 32) {
+        const unsigned long long* src = par_base + sidx;
+        unsigned long long wv[kRecBase];
+#pragma unroll
+        for (int w = 0; w < kRecBase; ++w) {
+          wv[w] = ld_relaxed_u64(src + w * st);
+          tags_ok = tags_ok && static_cast<unsigned>(wv[w] >> 32) == tag;
+        }
+        argmax_join(v2, i2, s2, join_hi_lo(wv[1], wv[2]), static_cast<int>(wv[0] & 0xffffffffu),
+                    static_cast<int>(wv[3] & 0xffffffffu));
+      }
+      if (has_pub) {
+        const unsigned long long* psrc = par_base + static_cast<size_t>(kRecBase + 2 * lane) * st + pub_owner[lane];
         pw0 = ld_relaxed_u64(psrc);
         pw1 = ld_relaxed_u64(psrc + st);
+        tags_ok = tags_ok && static_cast<unsigned>(pw0 >> 32) == tag && static_cast<unsigned>(pw1 >> 32) == tag;
       }
-#pragma unroll
-      for (int k = 0; k < kMaxPollPerLane; ++k) {
-        if (pending & (1u << k)) {
-          bool all = true;
-#pragma unroll
-          for (int w = 0; w < kRecBase; ++w) all = all && static_cast<unsigned>(wv[k][w] >> 32) == tag;
-          if (all) pending &= ~(1u << k);
-        }
+      if (!__all_sync(0xffffffffu, tags_ok)) {
+        if (lane == 0) fail(P.st, BBK_ERR_LOGIC);
+        ok = false;
       }
-      if (pub_pending && static_cast<unsigned>(pw0 >> 32) == tag && static_cast<unsigned>(pw1 >> 32) == tag)
-        pub_pending = false;
-      if (P.poll_ns && (pending || pub_pending)) __nanosleep(P.poll_ns);
-      if ((iter & 31u) == 0 && (pending || pub_pending)) {
-        if (ld_relaxed_s32(&P.st->abort)) {
-          ok = false;
-          break;
-        }
-        if (globaltimer_ns() - t0 > P.timeout_ns) {
-          fail(P.st, BBK_ERR_TIMEOUT);
-          ok = false;
-          break;
-        }
-      }
-    }
-    fence_acq_rel_gpu();  // acquire what the other CTAs released
-    double v = 0.0;
-    int i = INT_MAX, sl = -1;
-    if (ok) {
-      for (int k = 0; k < nmine; ++k)
-        argmax_join(v, i, sl, join_hi_lo(wv[k][1], wv[k][2]), static_cast<int>(wv[k][0] & 0xffffffffu),
-                    static_cast<int>(wv[k][3] & 0xffffffffu));
     }
     for (int off = 16; off > 0; off >>= 1) {
-      const double v2 = __shfl_down_sync(0xffffffffu, v, off);
-      const int i2 = __shfl_down_sync(0xffffffffu, i, off);
-      const int s2 = __shfl_down_sync(0xffffffffu, sl, off);
-      argmax_join(v, i, sl, v2, i2, s2);
+      const double v3 = __shfl_down_sync(0xffffffffu, v2, off);
+      const int i3 = __shfl_down_sync(0xffffffffu, i2, off);
+      const int s3 = __shfl_down_sync(0xffffffffu, s2, off);
+      argmax_join(v2, i2, s2, v3, i3, s3);
     }
     const int all_ok = __all_sync(0xffffffffu, ok);
     if (P.pub_ts && blockIdx.x == 0 && all_ok) {
-      // diagnostics: (last publish - own publish) and (done - last publish)
+      // diagnostics: (last arrival - own arrival) and (done - last arrival)
       const unsigned long long done = globaltimer_ns();
       unsigned long long last = 0;
       int who = 0;
@@ -275,9 +264,9 @@ __device__ void exchange(const PanelArgs& P, unsigned tag, double my_val, int my
     }
     if (has_pub) out->pub[lane] = join_hi_lo(pw0, pw1);
     if (lane == 0) {
-      out->val = v;
-      out->idx = i;
-      out->slot = sl;
+      out->val = v2;
+      out->idx = i2;
+      out->slot = s2;
       out->ok = all_ok;
     }
   }
@@ -377,7 +366,10 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
   cp_async_wait_all();
   __syncthreads();
 
-  unsigned tag = P.tag_base;
+  // exchanges are numbered across the factorization; the k-th (from 1) uses
+  // tag k and completes when the arrival counter reaches nslots * k
+  unsigned seq = static_cast<unsigned>(ldcg(&P.st->xseq[P.panel & 1]));
+  const unsigned long long nslots64 = static_cast<unsigned long long>(P.nslots);
   int p = kstart;
   // coefficients U[q, p] of the current row: rows q < n_old from the Uslot
   // column of p's slot, then lp - n_old (<= 2) values computed by every CTA.
@@ -451,7 +443,9 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
     owners[0] = owner(sp);
     owners[1] = lp + 1 < nwin ? owner(win[lp + 1]) : 0;
     owners[2] = lp + 2 < nwin ? owner(win[lp + 2]) : 0;
-    exchange(P, tag++, best, best_j, best_z, s_pub, owners, 3, s_red_v, s_red_i, s_red_s, &s_x);
+    const unsigned x1 = ++seq;
+    exchange(P, x1, nslots64 * x1, best, best_j, best_z, s_pub, owners, 3, s_red_v, s_red_i, s_red_s,
+             &s_x);
     if (!s_x.ok) return;
     const double omega = s_x.val;
     const int r = s_x.idx;
@@ -510,7 +504,8 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
       owners[1] = owner(sp);
       owners[2] = lp + 1 < nwin ? owner(win[lp + 1]) : 0;
       owners[3] = lp + 2 < nwin ? owner(win[lp + 2]) : 0;
-      exchange(P, tag++, sig, 0, 0, s_pub, owners, 4, s_red_v, s_red_i, s_red_s, &s_x);
+      const unsigned x2 = ++seq;
+      exchange(P, x2, nslots64 * x2, sig, 0, 0, s_pub, owners, 4, s_red_v, s_red_i, s_red_s, &s_x);
       if (!s_x.ok) return;
       const double sigma = s_x.val;
       wc_r = s_x.pub[0];
@@ -671,6 +666,7 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
   if (c == 0 && t == 0) {
     // panel range [kstart, e); the next panel starts at e.
     P.st->kstart[(P.panel + 1) & 1] = e;
+    P.st->xseq[(P.panel + 1) & 1] = static_cast<int>(seq + 1);  // + the barrier below
     if (P.panel_end) P.panel_end[P.panel] = e;
     if (P.stats) {
       for (int k = 0; k < 5; ++k) atomicAdd(P.stats + k, tm[k]);
@@ -681,7 +677,8 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
   // grid barrier: every CTA's maps and lists are visible after it
   {
     int owners0[kMaxPub] = {0, 0, 0, 0, 0, 0};
-    exchange(P, tag++, 0.0, 0, 0, s_pub, owners0, 0, s_red_v, s_red_i, s_red_s, &s_x);
+    const unsigned xb = ++seq;
+    exchange(P, xb, nslots64 * xb, 0.0, 0, 0, s_pub, owners0, 0, s_red_v, s_red_i, s_red_s, &s_x);
     if (!s_x.ok) return;
   }
   // ---- gather the interchanged data (written back by finalize_kernel)
@@ -816,6 +813,9 @@ __global__ void init_kernel(int n, int* perm, int* pivot_types, DeviceState* st,
     st->status = 0;
     st->moved[0] = 0;
     st->moved[1] = 0;
+    st->xseq[0] = 0;
+    st->xseq[1] = 0;
+    st->xcount = 0ull;
   }
 }
 
@@ -839,8 +839,9 @@ __global__ void __launch_bounds__(kThreads) probe_kernel(PanelArgs P) {
   __syncthreads();
   const unsigned long long t0 = globaltimer_ns();
   for (int it = 0; it < P.n; ++it) {
-    exchange(P, P.tag_base + it, static_cast<double>(blockIdx.x), blockIdx.x, blockIdx.x, s_pub, owners,
-             3, s_red_v, s_red_i, s_red_s, &s_x);
+    const unsigned x = static_cast<unsigned>(it) + 1u;
+    exchange(P, x, static_cast<unsigned long long>(P.nslots) * x, static_cast<double>(blockIdx.x),
+             blockIdx.x, blockIdx.x, s_pub, owners, 3, s_red_v, s_red_i, s_red_s, &s_x);
     if (!s_x.ok) return;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0 && P.stats) P.stats[0] = globaltimer_ns() - t0;
@@ -915,8 +916,6 @@ int launch_panel(const FactorPlan& plan, int panel, cudaStream_t s) {
   P.st = plan.state;
   P.nslots = plan.grid;
   P.slot_stride = plan.grid;
-  // tags: distinct for every exchange of the call (slots are zeroed per call)
-  P.tag_base = 1u + static_cast<unsigned>(panel) * (2u * static_cast<unsigned>(plan.b) + 8u);
   P.timeout_ns = plan.timeout_ns;
   P.stats = plan.stats;
   P.pub_ts = plan.stats ? plan.stats + 16 : nullptr;
@@ -925,8 +924,8 @@ int launch_panel(const FactorPlan& plan, int panel, cudaStream_t s) {
     return e ? static_cast<unsigned>(atoi(e)) : 0u;
   }();
   P.poll_ns = poll_ns;
-  if (plan.grid > 32 * kMaxPollPerLane)
-    return set_error(BBK_ERR_INVALID_ARGUMENT, "panel grid %d exceeds %d", plan.grid, 32 * kMaxPollPerLane);
+  if (plan.grid > kMaxGrid)
+    return set_error(BBK_ERR_INVALID_ARGUMENT, "panel grid %d exceeds %d", plan.grid, kMaxGrid);
   // shared memory: coefficient column + candidate column + (if it fits) the
   // slots' panel rows, then the window map and the slot -> index map
   const int smax = (plan.n + plan.grid - 1) / plan.grid;
@@ -988,7 +987,6 @@ int launch_probe_wait(int ctas, int nslots, int iters, unsigned long long timeou
   P.st = st;
   P.nslots = nslots;
   P.slot_stride = ctas + 1;
-  P.tag_base = 7u;
   P.timeout_ns = timeout_ns;
   P.n = iters;
   P.stats = stats;
