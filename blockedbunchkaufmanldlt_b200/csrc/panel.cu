@@ -40,16 +40,19 @@
 #include "bbk_internal.cuh"
 
 #ifndef BBK_PANEL_THREADS
-#define BBK_PANEL_THREADS 128
+#define BBK_PANEL_THREADS 192
 #endif
 
 namespace bbk {
 namespace {
 
 constexpr int kThreads = BBK_PANEL_THREADS;
-constexpr int kWarps = kThreads / 32;
-constexpr int kCols = 4;  // slots per thread: S <= kCols * kThreads
-constexpr int kMaxGrid = 256;  // CTAs of a panel launch (records per exchange)
+constexpr int kWarps = kThreads / 32;  // compute warps
+constexpr int kCommWarp = kWarps;       // the communication warp
+constexpr int kBlock = kThreads + 32;   // compute warps + the communication warp
+constexpr int kCols = 3;  // slots per thread: S <= kCols * kThreads
+constexpr int kMaxRecPerLane = 8;  // exchange records read per lane
+constexpr int kMaxGrid = 32 * kMaxRecPerLane;  // CTAs of a panel launch (records per exchange)
 constexpr int kRecBase = 4;  // record words before the published doubles: idx, hi, lo, slot
 static_assert(kRecBase + 2 * kMaxPub <= kSlotWords, "record too large");
 
@@ -132,9 +135,10 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // arrival counter reaches `target` (all `nslots` CTAs of this exchange), and
 // return the grid-wide argmax plus pub[k] taken from the record of CTA
 // pub_owner[k].  Must be called by every thread.
-__device__ void exchange(const PanelArgs& P, unsigned tag, unsigned long long target, double my_val,
-                         int my_idx, int my_slot, const double* pub_in, const int* pub_owner,
-                         int npub, double* s_red_v, int* s_red_i, int* s_red_s, ExchangeOut* out) {
+__device__ void exchange(const PanelArgs& P, unsigned tag, unsigned long long target, bool release,
+                         double my_val, int my_idx, int my_slot, const double* pub_in,
+                         const int* pub_owner, int npub, double* s_red_v, int* s_red_i, int* s_red_s,
+                         ExchangeOut* out) {
   const int t = threadIdx.x;
   const int lane = t & 31, warp = t >> 5;
   for (int off = 16; off > 0; off >>= 1) {
@@ -143,22 +147,23 @@ __device__ void exchange(const PanelArgs& P, unsigned tag, unsigned long long ta
     const int s2 = __shfl_down_sync(0xffffffffu, my_slot, off);
     argmax_join(my_val, my_idx, my_slot, v2, i2, s2);
   }
-  if (lane == 0) {
+  if (lane == 0 && warp < kWarps) {
     s_red_v[warp] = my_val;
     s_red_i[warp] = my_idx;
     s_red_s[warp] = my_slot;
   }
-  __syncthreads();  // also orders this CTA's global writes before the release
+  __syncthreads();  // also orders this CTA's global writes before a release
   // Structure-of-arrays records: word w of CTA c lives at
   // slots[((tag & 1) * kSlotWords + w) * slot_stride + c], so one warp load
   // reads word w of 32 consecutive CTAs in two cache lines.
   unsigned long long* par_base =
       P.slots + static_cast<size_t>(tag & 1u) * kSlotWords * P.slot_stride;
-  if (warp == 0) {
+  if (warp == kCommWarp) {
     double v = s_red_v[0];
     int i = s_red_i[0], sl = s_red_s[0];
     for (int k = 1; k < kWarps; ++k) argmax_join(v, i, sl, s_red_v[k], s_red_i[k], s_red_s[k]);
-    // one record word per lane: (tag | idx), (tag | hi v), (tag | lo v), (tag | slot), pubs
+    // one record word per lane: (tag | idx), (tag | hi v), (tag | lo v), (tag | slot), pubs;
+    // the tags tell a reader when each word has landed
     if (lane < kRecBase + 2 * npub) {
       unsigned word;
       if (lane == 0) {
@@ -174,14 +179,17 @@ __device__ void exchange(const PanelArgs& P, unsigned tag, unsigned long long ta
       st_relaxed_u64(par_base + static_cast<size_t>(lane) * P.slot_stride + blockIdx.x,
                      tag_word(tag, word));
     }
-    __syncwarp();
+    // Arrive.  The arrival must release what the CTA wrote for other CTAs
+    // (U columns); the panel issues that fence early, while the compute warps
+    // update the next row, and passes release = false here.
     if (lane == 0) {
+      if (release) fence_acq_rel_gpu();
       if (P.pub_ts) P.pub_ts[blockIdx.x] = globaltimer_ns();
-      // releases this CTA's record and everything the CTA wrote before it
-      red_release_add_u64(&P.st->xcount, 1ull);
+      red_relaxed_add_u64(&P.st->xcount, 1ull);
     }
     // Every lane polls the arrival counter (one request per warp load); the
-    // acquire load orders the record reads after it.
+    // acquire load orders the record reads (and, after the CTA barrier, the
+    // compute warps' reads of U) after it.
     const unsigned long long t0 = globaltimer_ns();
     bool ok = true;
     for (unsigned iter = 1;; ++iter) {
@@ -197,35 +205,55 @@ __device__ void exchange(const PanelArgs& P, unsigned tag, unsigned long long ta
         }
       }
     }
-    // one pass over the records (CTAs lane, lane+32, ...) and this lane's
-    // published word pair; the tags confirm every word is this exchange's
+    // Records of CTAs lane, lane+32, ... and this lane's published word pair,
+    // all loads of a pass issued together; a word whose tag is not yet this
+    // exchange's is read again (its store was issued after the arrival).
     const size_t st = P.slot_stride;
     double v2 = 0.0;
     int i2 = INT_MAX, s2 = -1;
     unsigned long long pw0 = 0, pw1 = 0;
     const bool has_pub = lane < npub;
     if (ok) {
-      bool tags_ok = true;
-      for (int sidx = lane; sidx < P.nslots; sidx += 32) {
-        const unsigned long long* src = par_base + sidx;
-        unsigned long long wv[kRecBase];
+      const int nmine = P.nslots > lane ? (P.nslots - lane + 31) / 32 : 0;  // <= kMaxRecPerLane
+      unsigned long long wv[kMaxRecPerLane][kRecBase];
+      const unsigned long long* psrc =
+          par_base + static_cast<size_t>(kRecBase + 2 * (has_pub ? lane : 0)) * st + (has_pub ? pub_owner[lane] : 0);
+      unsigned pending = (1u << nmine) - 1u;
+      bool pub_pending = has_pub;
+      for (unsigned iter = 1; pending || pub_pending; ++iter) {
 #pragma unroll
-        for (int w = 0; w < kRecBase; ++w) {
-          wv[w] = ld_relaxed_u64(src + w * st);
-          tags_ok = tags_ok && static_cast<unsigned>(wv[w] >> 32) == tag;
+        for (int k = 0; k < kMaxRecPerLane; ++k)
+          if (pending & (1u << k)) {
+            const unsigned long long* src = par_base + lane + 32 * k;
+#pragma unroll
+            for (int w = 0; w < kRecBase; ++w) wv[k][w] = __ldcg(src + w * st);
+          }
+        if (pub_pending) {
+          pw0 = __ldcg(psrc);
+          pw1 = __ldcg(psrc + st);
         }
-        argmax_join(v2, i2, s2, join_hi_lo(wv[1], wv[2]), static_cast<int>(wv[0] & 0xffffffffu),
-                    static_cast<int>(wv[3] & 0xffffffffu));
+#pragma unroll
+        for (int k = 0; k < kMaxRecPerLane; ++k)
+          if (pending & (1u << k)) {
+            bool all = true;
+#pragma unroll
+            for (int w = 0; w < kRecBase; ++w) all = all && static_cast<unsigned>(wv[k][w] >> 32) == tag;
+            if (all) pending &= ~(1u << k);
+          }
+        if (pub_pending && static_cast<unsigned>(pw0 >> 32) == tag && static_cast<unsigned>(pw1 >> 32) == tag)
+          pub_pending = false;
+        if ((iter & 31u) == 0 && (pending || pub_pending) && globaltimer_ns() - t0 > P.timeout_ns) {
+          fail(P.st, BBK_ERR_TIMEOUT);
+          ok = false;
+          break;
+        }
       }
-      if (has_pub) {
-        const unsigned long long* psrc = par_base + static_cast<size_t>(kRecBase + 2 * lane) * st + pub_owner[lane];
-        pw0 = ld_relaxed_u64(psrc);
-        pw1 = ld_relaxed_u64(psrc + st);
-        tags_ok = tags_ok && static_cast<unsigned>(pw0 >> 32) == tag && static_cast<unsigned>(pw1 >> 32) == tag;
-      }
-      if (!__all_sync(0xffffffffu, tags_ok)) {
-        if (lane == 0) fail(P.st, BBK_ERR_LOGIC);
-        ok = false;
+      if (ok) {
+#pragma unroll
+        for (int k = 0; k < kMaxRecPerLane; ++k)
+          if (k < nmine)
+            argmax_join(v2, i2, s2, join_hi_lo(wv[k][1], wv[k][2]), static_cast<int>(wv[k][0] & 0xffffffffu),
+                        static_cast<int>(wv[k][3] & 0xffffffffu));
       }
     }
     for (int off = 16; off > 0; off >>= 1) {
@@ -284,23 +312,54 @@ __device__ __forceinline__ double div_or_zero(double x, double den) {
 
 // sum_{q < count} c[q] * w(q) in ascending q, every product and sum rounded
 // separately (the reference's order).  The products do not depend on the
-// running sum, so they are issued eight at a time ahead of the serial adds.
+// running sum: each batch of eight is loaded and multiplied while the
+// previous batch is being added.
 template <typename WGet>
 __device__ __forceinline__ double ordered_dot(const double* c, int count, WGet&& w) {
   double acc = 0.0;
   int q = 0;
-  for (; q + 8 <= count; q += 8) {
-    double m[8];
+  if (count >= 8) {
+    double cur[8];
 #pragma unroll
-    for (int u = 0; u < 8; ++u) m[u] = xmul(c[q + u], w(q + u));
+    for (int u = 0; u < 8; ++u) cur[u] = xmul(c[u], w(u));
+    for (q = 8; q + 8 <= count; q += 8) {
+      double nxt[8];
 #pragma unroll
-    for (int u = 0; u < 8; ++u) acc = xadd(acc, m[u]);
+      for (int u = 0; u < 8; ++u) nxt[u] = xmul(c[q + u], w(q + u));
+#pragma unroll
+      for (int u = 0; u < 8; ++u) acc = xadd(acc, cur[u]);
+#pragma unroll
+      for (int u = 0; u < 8; ++u) cur[u] = nxt[u];
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) acc = xadd(acc, cur[u]);
   }
   for (; q < count; ++q) acc = xadd(acc, xmul(c[q], w(q)));
   return acc;
 }
 
-__global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
+// sum_{q < count} c[q] * w(q) with eight independent FMA accumulators
+// combined pairwise: the same sum, reassociated, with an eighth of the
+// dependent-latency chain (update modes that do not reproduce the
+// reference's rounding).
+template <typename WGet>
+__device__ __forceinline__ double split_dot(const double* c, int count, WGet&& w) {
+  double a[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  int q = 0;
+  for (; q + 8 <= count; q += 8) {
+#pragma unroll
+    for (int u = 0; u < 8; ++u) a[u] = __fma_rn(c[q + u], w(q + u), a[u]);
+  }
+#pragma unroll
+  for (int u = 0; u < 8; ++u)
+    if (q + u < count) a[u] = __fma_rn(c[q + u], w(q + u), a[u]);
+  return ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
+}
+
+// kOrdered: the row and candidate dot products in the reference's order
+// (bitwise the reference); otherwise reassociated (split_dot).
+template <bool kOrdered>
+__global__ void __launch_bounds__(kBlock) panel_kernel(PanelArgs P) {
   extern __shared__ double dsm[];
   __shared__ double s_red_v[kWarps];
   __shared__ int s_red_i[kWarps];
@@ -312,6 +371,9 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
   const int G = gridDim.x;
   const int c = blockIdx.x;
   const int t = threadIdx.x;
+  // slot-mapped work uses the compute threads only: the communication warp's
+  // tz puts its slots beyond every range
+  const int tz = t < kThreads ? t : (1 << 28);
   const int n = P.n;
   const int kstart = ldcg(&P.st->kstart[P.panel & 1]);
   const int S = (n - kstart + G - 1) / G;  // slots per CTA
@@ -350,10 +412,10 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
     }
   };
 
-  for (int m = t; m < nwin; m += kThreads) win[m] = kstart + m;
-  for (int zz = t; zz < width; zz += kThreads) mypos[zz] = lo + zz;
+  for (int m = t; m < nwin; m += kBlock) win[m] = kstart + m;
+  for (int zz = t; zz < width; zz += kBlock) mypos[zz] = lo + zz;
   // stage the panel rows of A for this CTA's slots
-  for (int idx = t; idx < nwin * width; idx += kThreads) {
+  for (int idx = t; idx < nwin * width; idx += kBlock) {
     const int m = idx / width, zz = idx - m * width;
     const int x = kstart + m, z = lo + zz;
     const double* src = x <= z ? P.a + static_cast<long long>(x) * lda + z
@@ -392,18 +454,18 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
     double av[kCols];
 #pragma unroll
     for (int k = 0; k < kCols; ++k) {
-      const int z = lo + t + k * kThreads;
+      const int z = lo + tz + k * kThreads;
       double v = 0.0;
       if (z < hi && mypos[z - lo] >= p) v = staged ? wat(lp, z) : asym(sp, z);
       av[k] = v;
     }
     {
       if (coef_pre) {
-        if (t < n_old) coef[t] = cpre[0];
-        if (t + kThreads < n_old) coef[t + kThreads] = cpre[1];
+        if (tz < n_old) coef[tz] = cpre[0];
+        if (tz + kThreads < n_old) coef[tz + kThreads] = cpre[1];
       } else {
         const double* ucol = P.uslot + static_cast<size_t>(sp) * ldu;
-        for (int q = t; q < n_old; q += kThreads) coef[q] = ldcg(ucol + q);
+        for (int q = t; q < n_old; q += kBlock) coef[q] = ldcg(ucol + q);
       }
       if (t == 0) {
         coef[n_old] = extra0;
@@ -412,15 +474,18 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
       if (t < kMaxPub) s_pub[t] = 0.0;
     }
     __syncthreads();
+    // release the previous step's U columns while the compute warps update the row
+    if (t == kThreads) fence_acq_rel_gpu();
     double best = 0.0;
     int best_j = INT_MAX, best_z = -1;
 #pragma unroll
     for (int k = 0; k < kCols; ++k) {
-      const int z = lo + t + k * kThreads;
+      const int z = lo + tz + k * kThreads;
       if (z < hi) {
         const int j = mypos[z - lo];
         if (j >= p) {
-          const double acc = ordered_dot(coef, lp, [&](int q) { return wat(q, z); });
+          const double acc = kOrdered ? ordered_dot(coef, lp, [&](int q) { return wat(q, z); })
+                                      : split_dot(coef, lp, [&](int q) { return wat(q, z); });
           const double wv = xsub(av[k], acc);
           wat(lp, z) = wv;
           if (j > p) {
@@ -444,8 +509,8 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
     owners[1] = lp + 1 < nwin ? owner(win[lp + 1]) : 0;
     owners[2] = lp + 2 < nwin ? owner(win[lp + 2]) : 0;
     const unsigned x1 = ++seq;
-    exchange(P, x1, nslots64 * x1, best, best_j, best_z, s_pub, owners, 3, s_red_v, s_red_i, s_red_s,
-             &s_x);
+    exchange(P, x1, nslots64 * x1, false, best, best_j, best_z, s_pub, owners, 3, s_red_v, s_red_i,
+             s_red_s, &s_x);
     if (!s_x.ok) return;
     const double omega = s_x.val;
     const int r = s_x.idx;
@@ -455,6 +520,20 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
     const double w_p2 = s_x.pub[2];  // W[p, p+2]
     __syncthreads();
     lap(1);
+    // The next row's coefficient column (rows q < lp, written before this
+    // step and visible since this exchange) is loaded now for every slot the
+    // next row may have, so its latency hides behind the rest of the step:
+    // A = slot of p+1, B = slot of p+2 (2x2 pivot), C = slot of p (r = p+1).
+    const bool prefetch = lp <= 2 * kThreads;
+    auto preload = [&](int slot, double& c0, double& c1) {
+      const double* ucol = P.uslot + static_cast<size_t>(slot) * ldu;
+      c0 = tz < lp ? ldcg(ucol + tz) : 0.0;
+      c1 = tz + kThreads < lp ? ldcg(ucol + tz + kThreads) : 0.0;
+    };
+    const int slot_a = lp + 1 < nwin ? win[lp + 1] : -1;
+    int slot_b = -1, slot_c = -1;
+    double ca0 = 0.0, ca1 = 0.0, cb0 = 0.0, cb1 = 0.0, cc0 = 0.0, cc1 = 0.0;
+    if (prefetch && slot_a >= 0) preload(slot_a, ca0, ca1);
 
     int kind = 1;  // 1: 1x1 at p; -1: 1x1 after p<->r; 2: 2x2 with p+1<->r
     bool cand = false;
@@ -463,28 +542,33 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
     if (!(fabs(dpp) >= xmul(kAlpha, omega) || omega == 0.0)) {
       cand = true;
       ++ncand;
+      slot_b = lp + 2 < nwin ? win[lp + 2] : -1;
+      slot_c = r == p + 1 ? sp : -1;
+      if (prefetch && slot_b >= 0) preload(slot_b, cb0, cb1);
+      if (prefetch && slot_c >= 0) preload(slot_c, cc0, cc1);
       // ---- candidate column W(i, r) = A(i, r) - sum_q U[q, r] W[q, i]
       // (CopyCandidateToWorkspace + UpdateCandidateInWorkspace, :184-352)
       double cv[kCols];
 #pragma unroll
       for (int k = 0; k < kCols; ++k) {
-        const int z = lo + t + k * kThreads;
+        const int z = lo + tz + k * kThreads;
         cv[k] = (z < hi && mypos[z - lo] >= p) ? asym(z, rs) : 0.0;
       }
       {
         const double* ucol = P.uslot + static_cast<size_t>(rs) * ldu;
-        for (int q = t; q < lp; q += kThreads) coef[q] = ldcg(ucol + q);
+        for (int q = t; q < lp; q += kBlock) coef[q] = ldcg(ucol + q);
         if (t < kMaxPub) s_pub[t] = 0.0;
       }
       __syncthreads();
       double sig = 0.0;
 #pragma unroll
       for (int k = 0; k < kCols; ++k) {
-        const int z = lo + t + k * kThreads;
+        const int z = lo + tz + k * kThreads;
         if (z < hi) {
           const int i = mypos[z - lo];
           if (i >= p) {
-            const double acc = ordered_dot(coef, lp, [&](int q) { return wat(q, z); });
+            const double acc = kOrdered ? ordered_dot(coef, lp, [&](int q) { return wat(q, z); })
+                                        : split_dot(coef, lp, [&](int q) { return wat(q, z); });
             const double v = xsub(cv[k], acc);
             wcs[z - lo] = v;
             if (i != r) {
@@ -505,7 +589,8 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
       owners[2] = lp + 1 < nwin ? owner(win[lp + 1]) : 0;
       owners[3] = lp + 2 < nwin ? owner(win[lp + 2]) : 0;
       const unsigned x2 = ++seq;
-      exchange(P, x2, nslots64 * x2, sig, 0, 0, s_pub, owners, 4, s_red_v, s_red_i, s_red_s, &s_x);
+      exchange(P, x2, nslots64 * x2, false, sig, 0, 0, s_pub, owners, 4, s_red_v, s_red_i, s_red_s,
+               &s_x);
       if (!s_x.ok) return;
       const double sigma = s_x.val;
       wc_r = s_x.pub[0];
@@ -534,7 +619,7 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
       const double den = safe_denominator(d);
 #pragma unroll
       for (int k = 0; k < kCols; ++k) {
-        const int z = lo + t + k * kThreads;
+        const int z = lo + tz + k * kThreads;
         if (z < hi) {
           const int j = mypos[z - lo];
           if (j > p) {
@@ -571,7 +656,7 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
       __syncthreads();
 #pragma unroll
       for (int k = 0; k < kCols; ++k) {
-        const int z = lo + t + k * kThreads;
+        const int z = lo + tz + k * kThreads;
         if (z < hi && mypos[z - lo] > p) {
           const double wv = wcs[z - lo];
           wat(lp, z) = wv;
@@ -605,7 +690,7 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
       __syncthreads();
 #pragma unroll
       for (int k = 0; k < kCols; ++k) {
-        const int z = lo + t + k * kThreads;
+        const int z = lo + tz + k * kThreads;
         if (z < hi && mypos[z - lo] > p + 1) {
           const double x = wat(lp, z);
           const double y = wcs[z - lo];
@@ -629,11 +714,21 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
       extra1 = xadd(xmul(i21, x), xmul(i22, y));
       p += 2;
     }
-    coef_pre = n_old <= 2 * kThreads && p < P.nominal_end;
+    coef_pre = prefetch && p < P.nominal_end;
     if (coef_pre) {
-      const double* ucol = P.uslot + static_cast<size_t>(win[p - kstart]) * ldu;
-      cpre[0] = t < n_old ? ldcg(ucol + t) : 0.0;
-      cpre[1] = t + kThreads < n_old ? ldcg(ucol + t + kThreads) : 0.0;
+      const int next = win[p - kstart];
+      if (next == slot_a) {
+        cpre[0] = ca0;
+        cpre[1] = ca1;
+      } else if (next == slot_b) {
+        cpre[0] = cb0;
+        cpre[1] = cb1;
+      } else if (next == slot_c) {
+        cpre[0] = cc0;
+        cpre[1] = cc1;
+      } else {
+        preload(next, cpre[0], cpre[1]);
+      }
     }
     __syncthreads();
     lap(4);
@@ -646,16 +741,16 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
   // ---- the panel's W and U in final column order, the slot of every index,
   // and the list of indices whose slot changed
   __syncthreads();
-  for (int idx = t; idx < width * kb; idx += kThreads) {
+  for (int idx = t; idx < width * kb; idx += kBlock) {
     const int zz = idx / kb, q = idx - zz * kb;
     P.ucm[static_cast<size_t>(mypos[zz]) * ldu + q] = P.uslot[static_cast<size_t>(lo + zz) * ldu + q];
   }
-  for (int idx = t; idx < width * kb; idx += kThreads) {
+  for (int idx = t; idx < width * kb; idx += kBlock) {
     const int q = idx / width, zz = idx - q * width;
     const int x = mypos[zz];
     if (x >= e) P.w[q * ldw + x] = wat(q, lo + zz);
   }
-  for (int zz = t; zz < width; zz += kThreads) {
+  for (int zz = t; zz < width; zz += kBlock) {
     const int x = mypos[zz], z = lo + zz;
     P.srcmap[x] = z;
     if (x != z) {
@@ -678,7 +773,7 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
   {
     int owners0[kMaxPub] = {0, 0, 0, 0, 0, 0};
     const unsigned xb = ++seq;
-    exchange(P, xb, nslots64 * xb, 0.0, 0, 0, s_pub, owners0, 0, s_red_v, s_red_i, s_red_s, &s_x);
+    exchange(P, xb, nslots64 * xb, true, 0.0, 0, 0, s_pub, owners0, 0, s_red_v, s_red_i, s_red_s, &s_x);
     if (!s_x.ok) return;
   }
   // ---- gather the interchanged data (written back by finalize_kernel)
@@ -686,8 +781,8 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(PanelArgs P) {
   if (cnt == 0) return;
   const int* list = P.moved + (P.panel & 1) * P.move_cap;
   const long long m = n - kstart;
-  const long long nthreads = static_cast<long long>(G) * kThreads;
-  const long long gtid = static_cast<long long>(c) * kThreads + t;
+  const long long nthreads = static_cast<long long>(G) * kBlock;
+  const long long gtid = static_cast<long long>(c) * kBlock + t;
   // rows of the moved indices over the active columns: gbuf[ix][y - k0] = A(src x, src y)
   for (long long idx = gtid; idx < cnt * m; idx += nthreads) {
     const int ix = static_cast<int>(idx / m);
@@ -828,7 +923,7 @@ __global__ void status_copy_kernel(const DeviceState* st, int* out) {
 // bounded-wait test).  With nslots == gridDim.x it runs `iters` exchanges
 // back to back and CTA 0 stores the elapsed nanoseconds in stats[0] (the
 // exchange-latency measurement).
-__global__ void __launch_bounds__(kThreads) probe_kernel(PanelArgs P) {
+__global__ void __launch_bounds__(kBlock) probe_kernel(PanelArgs P) {
   __shared__ double s_red_v[kWarps];
   __shared__ int s_red_i[kWarps];
   __shared__ int s_red_s[kWarps];
@@ -840,7 +935,7 @@ __global__ void __launch_bounds__(kThreads) probe_kernel(PanelArgs P) {
   const unsigned long long t0 = globaltimer_ns();
   for (int it = 0; it < P.n; ++it) {
     const unsigned x = static_cast<unsigned>(it) + 1u;
-    exchange(P, x, static_cast<unsigned long long>(P.nslots) * x, static_cast<double>(blockIdx.x),
+    exchange(P, x, static_cast<unsigned long long>(P.nslots) * x, true, static_cast<double>(blockIdx.x),
              blockIdx.x, blockIdx.x, s_pub, owners, 3, s_red_v, s_red_i, s_red_s, &s_x);
     if (!s_x.ok) return;
   }
@@ -851,7 +946,7 @@ __global__ void __launch_bounds__(kThreads) probe_kernel(PanelArgs P) {
 
 static int cooperative_launch(const void* fn, int grid, PanelArgs* args, cudaStream_t s) {
   void* kargs[] = {args};
-  cudaError_t err = cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kThreads), kargs, 0, s);
+  cudaError_t err = cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kBlock), kargs, 0, s);
   if (err != cudaSuccess) return cuda_error(err, "cudaLaunchCooperativeKernel(panel)");
   count_launch();
   return BBK_OK;
@@ -937,11 +1032,12 @@ int launch_panel(const FactorPlan& plan, int panel, cudaStream_t s) {
   const size_t limit = 220 * 1024;
   P.w_smem = base + wbytes <= limit;
   const size_t bytes = base + (P.w_smem ? wbytes : 0);
-  BBK_CUDA_TRY(cudaFuncSetAttribute(panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    static_cast<int>(bytes)));
+  const void* fn = plan.mode == BBK_UPDATE_FP64_ORDERED
+                       ? reinterpret_cast<const void*>(panel_kernel<true>)
+                       : reinterpret_cast<const void*>(panel_kernel<false>);
+  BBK_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)));
   void* kargs[] = {&P};
-  cudaError_t err = cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(panel_kernel),
-                                                dim3(plan.grid), dim3(kThreads), kargs, bytes, s);
+  cudaError_t err = cudaLaunchCooperativeKernel(fn, dim3(plan.grid), dim3(kBlock), kargs, bytes, s);
   if (err != cudaSuccess) return cuda_error(err, "cudaLaunchCooperativeKernel(panel)");
   count_launch();
   return BBK_OK;
