@@ -51,6 +51,7 @@ EXPORTS = (
     "bbk_reconstruct_device", "bbk_scale_one_by_one", "bbk_scale_two_by_two",
     "bbk_update_trailing_block", "bbk_profile_begin", "bbk_profile_end", "bbk_panel_stats", "bbk_panel_stats_raw", "bbk_solve_device_noalloc",
     "bbk_solve_refined_workspace_size", "bbk_solve_refined_device",
+    "bbk_batched_workspace_size", "bbk_batched_plan", "bbk_batched_factor_solve",
 )
 
 
@@ -60,6 +61,19 @@ class RefineInfo(ctypes.Structure):
                 ("converged", ctypes.c_int), ("reserved", ctypes.c_int),
                 ("initial_backward_error", ctypes.c_double), ("backward_error", ctypes.c_double)]
 SOLVE_NOALLOC_MAX_ELEMENTS = 524288  # n * nrhs limit of bbk_solve_device_noalloc
+BATCH_MAX_N = 1024                  # largest order of a batched item
+BATCH_BUCKETS = 6                   # block-size buckets: n <= 32, 64, 128, 256, 512, 1024
+
+
+class BatchItem(ctypes.Structure):
+    """bbk_batch_item"""
+    _fields_ = [("n", ctypes.c_int), ("lda", ctypes.c_int), ("a", ctypes.c_longlong),
+                ("rhs", ctypes.c_longlong), ("piv", ctypes.c_longlong)]
+
+
+class BatchInfo(ctypes.Structure):
+    """bbk_batch_info"""
+    _fields_ = [("iterations", ctypes.c_int), ("converged", ctypes.c_int), ("backward_error", ctypes.c_double)]
 PROFILE_CLASSES = ("init", "panel", "finalize", "update", "solve")
 
 
@@ -126,6 +140,10 @@ def lib() -> ctypes.CDLL:
         "bbk_solve_host": ([_c_int, _vp, _c_ll, _vp, _vp, _c_int, _vp, _c_ll], _c_int),
         "bbk_solve_device_noalloc": ([_c_int, _vp, _c_ll, _vp, _vp, _c_int, _vp, _c_ll, _vp], _c_int),
         "bbk_solve_refined_workspace_size": ([_c_int, _c_int, _c_int], _c_sz),
+        "bbk_batched_workspace_size": ([_c_int, _c_int], _c_sz),
+        "bbk_batched_plan": ([_c_int, _vp, _vp, _vp, _vp, _c_sz, _vp], _c_int),
+        "bbk_batched_factor_solve": ([_c_int, _vp, _vp, _vp, _vp, _vp, _c_int, ctypes.c_double, _c_int, _vp,
+                                      _vp, _c_sz, _vp], _c_int),
         "bbk_solve_refined_device": ([_c_int, _vp, _c_ll, _vp, _c_ll, _vp, _vp, _c_int, _vp, _c_ll, _vp,
                                       _c_ll, ctypes.c_double, _c_int, _c_int, _c_int, _vp, _vp, _c_sz,
                                       _vp], _c_int),
@@ -428,3 +446,96 @@ class BlockLdltDecomposition:
 
     def solve(self, b: np.ndarray) -> np.ndarray:
         return solve_host(self._need(), b)
+
+
+# ---------------------------------------------------------------------------
+# Batched factor + solve
+# ---------------------------------------------------------------------------
+class BatchedPlan:
+    """A planned batch: packed layout of `sizes` (matrix k is n_k x n_k at
+    element offset a_offsets[k], its right-hand side at rhs_offsets[k], its
+    perm / pivot types at piv_offsets[k]), the block size chosen per item
+    and the device workspace holding the schedule."""
+
+    def __init__(self, sizes, block_sizes=None, device=None, stream=None):
+        import torch
+        sizes = [int(n) for n in sizes]
+        if not sizes:
+            raise InvalidArgument(BBK_ERR_INVALID_ARGUMENT, "empty batch")
+        self.sizes = np.asarray(sizes, dtype=np.int64)
+        self.count = len(sizes)
+        self.a_offsets = np.concatenate([[0], np.cumsum(self.sizes * self.sizes)[:-1]]).astype(np.int64)
+        self.rhs_offsets = np.concatenate([[0], np.cumsum(self.sizes)[:-1]]).astype(np.int64)
+        self.piv_offsets = self.rhs_offsets.copy()
+        self.a_elements = int((self.sizes * self.sizes).sum())
+        self.vec_elements = int(self.sizes.sum())
+        items = (BatchItem * self.count)()
+        for k, n in enumerate(sizes):
+            items[k].n = n
+            items[k].lda = n
+            items[k].a = int(self.a_offsets[k])
+            items[k].rhs = int(self.rhs_offsets[k])
+            items[k].piv = int(self.piv_offsets[k])
+        self.device = device if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.bytes = lib().bbk_batched_workspace_size(self.count, max(sizes))
+        if self.bytes == 0:
+            raise InvalidArgument(BBK_ERR_INVALID_ARGUMENT, "batched sizes outside 1..%d" % BATCH_MAX_N)
+        self.workspace = torch.empty(self.bytes, dtype=torch.uint8, device=self.device)
+        chosen = np.zeros(self.count, dtype=np.int32)
+        table = None
+        if block_sizes is not None:
+            bs = np.zeros(BATCH_BUCKETS, dtype=np.int32)
+            bs[:len(block_sizes)] = np.asarray(block_sizes, dtype=np.int32)
+            table = bs
+        check(lib().bbk_batched_plan(self.count, ctypes.cast(items, ctypes.c_void_p),
+                                     _np_ptr(table) if table is not None else None, _np_ptr(chosen),
+                                     ctypes.c_void_p(self.workspace.data_ptr()), self.bytes, _stream_ptr(stream)))
+        self.block_sizes = chosen
+
+    def pack(self, mats, vecs=None):
+        """Host lists of square matrices / vectors -> packed CUDA tensors."""
+        import torch
+        a = np.empty(self.a_elements)
+        for k, m in enumerate(mats):
+            o = int(self.a_offsets[k])
+            a[o:o + m.size] = np.ascontiguousarray(m, dtype=np.float64).ravel()
+        out = [torch.from_numpy(a).to(self.device)]
+        if vecs is not None:
+            x = np.empty(self.vec_elements)
+            for k, v in enumerate(vecs):
+                o = int(self.rhs_offsets[k])
+                x[o:o + v.size] = np.asarray(v, dtype=np.float64).ravel()
+            out.append(torch.from_numpy(x).to(self.device))
+        return out
+
+    def matrix(self, a, k):
+        n = int(self.sizes[k])
+        o = int(self.a_offsets[k])
+        return a[o:o + n * n].reshape(n, n)
+
+    def vector(self, x, k):
+        o = int(self.rhs_offsets[k])
+        return x[o:o + int(self.sizes[k])]
+
+
+def batched_factor_solve(plan: BatchedPlan, a, x, mode="fp64", a_orig=None, tol: float = 1e-12,
+                         max_iter: int = 0, stream=None, sync: bool = True):
+    """Factor every matrix of the packed CUDA float64 tensor ``a`` in place and
+    solve into ``x`` (overwritten).  Returns (perm, pivot_types, info) device
+    tensors; info is a structured numpy array when ``sync``."""
+    import torch
+    perm = torch.empty(plan.vec_elements, dtype=torch.int32, device=plan.device)
+    pt = torch.empty(plan.vec_elements, dtype=torch.int32, device=plan.device)
+    info = torch.zeros(plan.count * ctypes.sizeof(BatchInfo), dtype=torch.uint8, device=plan.device)
+    check(lib().bbk_batched_factor_solve(
+        plan.count, ctypes.c_void_p(a.data_ptr()), ctypes.c_void_p(a_orig.data_ptr()) if a_orig is not None else None,
+        ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(perm.data_ptr()), ctypes.c_void_p(pt.data_ptr()),
+        _mode(mode), float(tol), int(max_iter), ctypes.c_void_p(info.data_ptr()),
+        ctypes.c_void_p(plan.workspace.data_ptr()), plan.bytes, _stream_ptr(stream)))
+    if not sync:
+        return perm, pt, info
+    torch.cuda.synchronize(plan.device)
+    raw = info.cpu().numpy().tobytes()
+    rec = np.frombuffer(raw, dtype=np.dtype([("iterations", "<i4"), ("converged", "<i4"),
+                                             ("backward_error", "<f8")]))
+    return perm, pt, rec

@@ -18,6 +18,7 @@ int cuda_error(cudaError_t err, const char* what);
 void count_launch(unsigned n = 1);
 unsigned long long wait_timeout_ns();
 int device_sm_count();
+int check_device();  // BBK_OK on an sm_10x device, else BBK_ERR_NO_DEVICE
 
 #define BBK_CUDA_TRY(expr)                                            \
   do {                                                                \
@@ -78,6 +79,65 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
+}
+
+// ---------------------------------------------------------------------------
+// Pivot arithmetic shared by the panel and batched kernels
+// (src/block_ldlt_decomposition.cc in wentianshu/BlockedBunchKaufmanLDLT)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double safe_denominator(double d) {
+  // src/block_ldlt_decomposition.cc:21-26 (absolute threshold)
+  return fabs(d) <= kDblEpsilon ? 0.0 : d;
+}
+
+__device__ __forceinline__ double div_or_zero(double x, double den) {
+  return den == 0.0 ? 0.0 : xdiv(x, den);
+}
+
+// sum_{q < count} c[q] * w(q) in ascending q, every product and sum rounded
+// separately (the reference's order).  The products do not depend on the
+// running sum: each batch of eight is loaded and multiplied while the
+// previous batch is being added.
+template <typename WGet>
+__device__ __forceinline__ double ordered_dot(const double* c, int count, WGet&& w) {
+  double acc = 0.0;
+  int q = 0;
+  if (count >= 8) {
+    double cur[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) cur[u] = xmul(c[u], w(u));
+    for (q = 8; q + 8 <= count; q += 8) {
+      double nxt[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) nxt[u] = xmul(c[q + u], w(q + u));
+#pragma unroll
+      for (int u = 0; u < 8; ++u) acc = xadd(acc, cur[u]);
+#pragma unroll
+      for (int u = 0; u < 8; ++u) cur[u] = nxt[u];
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) acc = xadd(acc, cur[u]);
+  }
+  for (; q < count; ++q) acc = xadd(acc, xmul(c[q], w(q)));
+  return acc;
+}
+
+// sum_{q < count} c[q] * w(q) with eight independent FMA accumulators
+// combined pairwise: the same sum, reassociated, with an eighth of the
+// dependent-latency chain (update modes that do not reproduce the
+// reference's rounding).
+template <typename WGet>
+__device__ __forceinline__ double split_dot(const double* c, int count, WGet&& w) {
+  double a[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  int q = 0;
+  for (; q + 8 <= count; q += 8) {
+#pragma unroll
+    for (int u = 0; u < 8; ++u) a[u] = __fma_rn(c[q + u], w(q + u), a[u]);
+  }
+#pragma unroll
+  for (int u = 0; u < 8; ++u)
+    if (q + u < count) a[u] = __fma_rn(c[q + u], w(q + u), a[u]);
+  return ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
 }
 
 // Device status words shared by every kernel of one factorization.

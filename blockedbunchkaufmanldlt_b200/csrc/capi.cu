@@ -55,18 +55,6 @@ int profiled(int cls, cudaStream_t s, F&& launch) {
   return rc;
 }
 
-int check_device() {
-  int dev = 0;
-  cudaError_t err = cudaGetDevice(&dev);
-  if (err != cudaSuccess) return set_error(BBK_ERR_NO_DEVICE, "no CUDA device: %s", cudaGetErrorString(err));
-  int major = 0;
-  err = cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
-  if (err != cudaSuccess) return cuda_error(err, "cudaDeviceGetAttribute");
-  if (major != 10)
-    return set_error(BBK_ERR_NO_DEVICE,
-                     "libbbk_b200 is built for sm_100a only; device %d is sm_%d0", dev, major);
-  return BBK_OK;
-}
 
 struct Carver {
   char* base;
@@ -135,6 +123,19 @@ int set_error(int status, const char* fmt, ...) {
 int cuda_error(cudaError_t err, const char* what) {
   snprintf(g_error, sizeof(g_error), "%s: %s", what, cudaGetErrorString(err));
   return err == cudaErrorMemoryAllocation ? BBK_ERR_ALLOC : BBK_ERR_CUDA;
+}
+
+int check_device() {
+  int dev = 0;
+  cudaError_t err = cudaGetDevice(&dev);
+  if (err != cudaSuccess) return set_error(BBK_ERR_NO_DEVICE, "no CUDA device: %s", cudaGetErrorString(err));
+  int major = 0;
+  err = cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+  if (err != cudaSuccess) return cuda_error(err, "cudaDeviceGetAttribute");
+  if (major != 10)
+    return set_error(BBK_ERR_NO_DEVICE,
+                     "libbbk_b200 is built for sm_100a only; device %d is sm_%d0", dev, major);
+  return BBK_OK;
 }
 
 void count_launch(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }

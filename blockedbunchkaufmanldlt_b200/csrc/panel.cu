@@ -301,61 +301,6 @@ __device__ void exchange(const PanelArgs& P, unsigned tag, unsigned long long ta
   __syncthreads();
 }
 
-__device__ __forceinline__ double safe_denominator(double d) {
-  // src/block_ldlt_decomposition.cc:21-26 (absolute threshold)
-  return fabs(d) <= kDblEpsilon ? 0.0 : d;
-}
-
-__device__ __forceinline__ double div_or_zero(double x, double den) {
-  return den == 0.0 ? 0.0 : xdiv(x, den);
-}
-
-// sum_{q < count} c[q] * w(q) in ascending q, every product and sum rounded
-// separately (the reference's order).  The products do not depend on the
-// running sum: each batch of eight is loaded and multiplied while the
-// previous batch is being added.
-template <typename WGet>
-__device__ __forceinline__ double ordered_dot(const double* c, int count, WGet&& w) {
-  double acc = 0.0;
-  int q = 0;
-  if (count >= 8) {
-    double cur[8];
-#pragma unroll
-    for (int u = 0; u < 8; ++u) cur[u] = xmul(c[u], w(u));
-    for (q = 8; q + 8 <= count; q += 8) {
-      double nxt[8];
-#pragma unroll
-      for (int u = 0; u < 8; ++u) nxt[u] = xmul(c[q + u], w(q + u));
-#pragma unroll
-      for (int u = 0; u < 8; ++u) acc = xadd(acc, cur[u]);
-#pragma unroll
-      for (int u = 0; u < 8; ++u) cur[u] = nxt[u];
-    }
-#pragma unroll
-    for (int u = 0; u < 8; ++u) acc = xadd(acc, cur[u]);
-  }
-  for (; q < count; ++q) acc = xadd(acc, xmul(c[q], w(q)));
-  return acc;
-}
-
-// sum_{q < count} c[q] * w(q) with eight independent FMA accumulators
-// combined pairwise: the same sum, reassociated, with an eighth of the
-// dependent-latency chain (update modes that do not reproduce the
-// reference's rounding).
-template <typename WGet>
-__device__ __forceinline__ double split_dot(const double* c, int count, WGet&& w) {
-  double a[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  int q = 0;
-  for (; q + 8 <= count; q += 8) {
-#pragma unroll
-    for (int u = 0; u < 8; ++u) a[u] = __fma_rn(c[q + u], w(q + u), a[u]);
-  }
-#pragma unroll
-  for (int u = 0; u < 8; ++u)
-    if (q + u < count) a[u] = __fma_rn(c[q + u], w(q + u), a[u]);
-  return ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
-}
-
 // kOrdered: the row and candidate dot products in the reference's order
 // (bitwise the reference); otherwise reassociated (split_dot).
 template <bool kOrdered>

@@ -46,11 +46,14 @@ typedef enum bbk_status {
   BBK_ERR_WORKSPACE = 8         /* caller workspace smaller than required */
 } bbk_status;
 
-/* Arithmetic of the trailing update A22 -= U^T W.  The panel (pivot search,
- * interchanges, scaling, in-panel row updates) is always FP64 in the
- * reference's own operation order. */
+/* Arithmetic of the factorization.  The panel (pivot search, interchanges,
+ * scaling, in-panel row updates) is always FP64, with the 1x1/2x2 tests,
+ * determinants and divisions in the reference's own operation order; its
+ * in-panel dot products keep the reference's summation order only in
+ * BBK_UPDATE_FP64_ORDERED (elsewhere they are reassociated FMA chains). */
 typedef enum bbk_update_mode {
-  BBK_UPDATE_FP64 = 0,         /* FP64 tensor cores (DMMA mma.sync f64) */
+  BBK_UPDATE_FP64 = 0,         /* FP64 tensor cores (DMMA mma.sync f64) for the
+                                  trailing update */
   BBK_UPDATE_FP64_ORDERED = 1, /* FP64, reference summation order: bitwise
                                   identical to the reference */
   BBK_UPDATE_FP32 = 2,         /* operands rounded to FP32, FP32 accumulate,
@@ -246,6 +249,61 @@ int bbk_update_trailing_block(int rows, int cols, int inner_dim,
                               int workspace_panel_stride, double* target,
                               int target_stride, int update_mode,
                               void* stream);
+
+/* ---------------------------------------------------------------------------
+ * Batched factor + solve: many independent small symmetric matrices, each
+ * factored with the reference's blocked Bunch-Kaufman algorithm
+ * (BlockLdltDecomposition::Factorize, src/block_ldlt_decomposition.cc:
+ * 28-78) and solved for one right-hand side, all in one persistent launch
+ * (one CTA per matrix at a time, largest matrices first).  No reference
+ * counterpart as a batch: the reference factors one matrix per object.
+ *
+ * Buffers are device memory.  Item k's matrix is n x lda row-major at
+ * a + items[k].a (upper triangle read; compact factors written in place),
+ * its right-hand side at x + items[k].rhs (overwritten by the solution), and
+ * its perm / pivot_types at perm + items[k].piv / pivot_types +
+ * items[k].piv.  Block sizes are chosen per size bucket (n <= 32, 64, 128,
+ * 256, 512, 1024); the library clamps each to what shared memory holds.
+ * ------------------------------------------------------------------------- */
+#define BBK_BATCH_MAX_N 1024
+#define BBK_BATCH_BUCKETS 6
+typedef struct bbk_batch_item {
+  int n;          /* order, 1..BBK_BATCH_MAX_N */
+  int lda;        /* leading dimension, >= n */
+  long long a;    /* element offset of the matrix in the a buffer */
+  long long rhs;  /* element offset of the right-hand side in the x buffer */
+  long long piv;  /* element offset of perm / pivot_types entries */
+} bbk_batch_item;
+
+typedef struct bbk_batch_info {
+  int iterations;        /* refinement steps taken (0 without refinement) */
+  int converged;         /* 1: backward error <= tol (always 1 without refinement) */
+  double backward_error; /* max|b - A x| / (||A||_inf ||x||_inf + ||b||_inf) (refined modes) */
+} bbk_batch_info;
+
+/* Bytes of workspace for `count` items whose largest order is max_n. */
+size_t bbk_batched_workspace_size(int count, int max_n);
+/* Set-up (host, synchronous on `stream`): sorts the items largest first,
+ * picks each item's block size from block_sizes[bucket] (NULL or 0 entries:
+ * built-in defaults; BBK_BATCH_BUCKETS entries), writes the block size used
+ * for item k to chosen_blocks[k] when that array is non-NULL, and stores the
+ * schedule in the workspace. */
+int bbk_batched_plan(int count, const bbk_batch_item* items_host,
+                     const int* block_sizes, int* chosen_blocks,
+                     void* workspace, size_t workspace_bytes, void* stream);
+/* Factor and solve every planned item (asynchronous, allocates nothing; the
+ * launch sequence can be captured in a CUDA graph).  update_mode:
+ * BBK_UPDATE_FP64_ORDERED (the reference's arithmetic bit for bit),
+ * BBK_UPDATE_FP64, or BBK_UPDATE_FP32 (FP32 trailing updates; with a_orig
+ * non-NULL and max_iter > 0 the solution is refined in FP64 against the
+ * original matrices at a_orig + items[k].a until the backward error is <=
+ * tol).  info (device, optional) receives one record per item, in the
+ * caller's item order. */
+int bbk_batched_factor_solve(int count, double* a, const double* a_orig,
+                             double* x, int* perm, int* pivot_types,
+                             int update_mode, double tol, int max_iter,
+                             bbk_batch_info* info, void* workspace,
+                             size_t workspace_bytes, void* stream);
 
 #ifdef __cplusplus
 }
