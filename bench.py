@@ -84,6 +84,31 @@ def workload_config(args, n_used=None) -> dict:
 
 
 # ---------------------------------------------------------------------------
+# multi-process helpers (one process per GPU; NCCL on GPUs, gloo in the CPU tests)
+# ---------------------------------------------------------------------------
+def reduce_max_over_ranks(value: float, world: int, device) -> float:
+    """The maximum of `value` over all ranks of the default process group
+    (every rank calls it the same number of times, in the same order)."""
+    if world <= 1:
+        return float(value)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(units_per_rank: float, world: int, max_ms: float) -> float:
+    """Whole-job rate: every rank's units over the slowest rank's time."""
+    return world * units_per_rank / (max_ms / 1e3)
+
+
+def batch_seed(seed: int, rank: int) -> int:
+    """Each rank of the batched workload owns its own seeded batch."""
+    return seed + 1000 * rank
+
+
+# ---------------------------------------------------------------------------
 # clocks sampling (nvidia-smi during the timed region)
 # ---------------------------------------------------------------------------
 class ClockSampler:
@@ -240,11 +265,7 @@ def run_b200(args):
             dist.barrier()
 
     def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max_over_ranks(x, world, dev)
 
     n, blk, nrhs = args.n, args.block, args.nrhs
     h = args.h if args.h is not None else int(round(0.8 * n))
@@ -612,13 +633,9 @@ def run_batched(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
 
     def max_over_ranks(v: float) -> float:
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max_over_ranks(v, world, dev)
 
-    seed = args.seed + 1000 * rank  # weak scaling: every rank owns its own batch
+    seed = batch_seed(args.seed, rank)  # weak scaling: every rank owns its own batch
     sizes = batched_sizes(args.count, seed)
     table = tuning.load_table()
     plan = bbk.BatchedPlan(sizes, block_sizes=table)
