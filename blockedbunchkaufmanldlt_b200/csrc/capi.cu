@@ -135,6 +135,18 @@ int check_device() {
   if (major != 10)
     return set_error(BBK_ERR_NO_DEVICE,
                      "libbbk_b200 is built for sm_100a only; device %d is sm_%d0", dev, major);
+  // Workspace this library allocates with cudaMallocAsync goes back to the
+  // device's default pool; keep it there instead of releasing it to the
+  // driver at every synchronization, so repeated calls reuse it.
+  static bool pool_kept[64] = {};
+  if (dev >= 0 && dev < 64 && !pool_kept[dev]) {
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+      unsigned long long keep = ~0ull;  // the attribute is a 64-bit byte count
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    pool_kept[dev] = true;
+  }
   return BBK_OK;
 }
 
