@@ -125,6 +125,24 @@ int cuda_error(cudaError_t err, const char* what) {
   return err == cudaErrorMemoryAllocation ? BBK_ERR_ALLOC : BBK_ERR_CUDA;
 }
 
+// Copies the upper triangle of an n x ld row-major matrix between host and
+// device as 64-row block wedges (rows [k, k+64), columns [k, n)): about half
+// the bytes of the full matrix.  The few strictly-lower entries inside each
+// wedge are copied unchanged (the factorization never writes them).
+cudaError_t copy_upper(double* dst, const double* src, int n, long long ld, cudaMemcpyKind kind,
+                       cudaStream_t s) {
+  constexpr int kRows = 64;
+  const size_t pitch = static_cast<size_t>(ld) * sizeof(double);
+  for (int k = 0; k < n; k += kRows) {
+    const int h = n - k < kRows ? n - k : kRows;
+    const size_t off = static_cast<size_t>(k) * ld + k;
+    cudaError_t err = cudaMemcpy2DAsync(dst + off, pitch, src + off, pitch,
+                                        static_cast<size_t>(n - k) * sizeof(double), h, kind, s);
+    if (err != cudaSuccess) return err;
+  }
+  return cudaSuccess;
+}
+
 int check_device() {
   int dev = 0;
   cudaError_t err = cudaGetDevice(&dev);
@@ -428,7 +446,7 @@ int bbk_solve_host(int n, const double* factors, long long ldf, const int* perm,
   if (err == cudaSuccess) err = cudaMallocAsync(reinterpret_cast<void**>(&d_pt), n * sizeof(int), s);
   if (err == cudaSuccess)
     err = cudaMallocAsync(reinterpret_cast<void**>(&work), bbk_solve_workspace_size(n, nrhs), s);
-  if (err == cudaSuccess) err = cudaMemcpyAsync(d_f, factors, fbytes, cudaMemcpyHostToDevice, s);
+  if (err == cudaSuccess) err = copy_upper(d_f, factors, n, ldf, cudaMemcpyHostToDevice, s);
   if (err == cudaSuccess) err = cudaMemcpyAsync(d_b, b, bbytes, cudaMemcpyHostToDevice, s);
   if (err == cudaSuccess) err = cudaMemcpyAsync(d_perm, perm, n * sizeof(int), cudaMemcpyHostToDevice, s);
   if (err == cudaSuccess) err = cudaMemcpyAsync(d_pt, pivot_types, n * sizeof(int), cudaMemcpyHostToDevice, s);
@@ -479,7 +497,7 @@ int bbk_factor_solve_host(int n, int block_size, double* a, long long lda, int* 
   if (err == cudaSuccess) err = cudaMallocAsync(reinterpret_cast<void**>(&d_status), sizeof(int), s);
   if (err == cudaSuccess)
     err = cudaMallocAsync(reinterpret_cast<void**>(&ws), fws > sws ? fws : sws, s);
-  if (err == cudaSuccess) err = cudaMemcpyAsync(d_a, a, abytes, cudaMemcpyHostToDevice, s);
+  if (err == cudaSuccess) err = copy_upper(d_a, a, n, lda, cudaMemcpyHostToDevice, s);
   if (err == cudaSuccess && nrhs > 0) err = cudaMemcpyAsync(d_b, b, bbytes, cudaMemcpyHostToDevice, s);
   if (err != cudaSuccess) {
     rc = cuda_error(err, "factorization setup");
@@ -489,7 +507,7 @@ int bbk_factor_solve_host(int n, int block_size, double* a, long long lda, int* 
     if (!rc && nrhs > 0) rc = enqueue_solve(n, d_a, lda, d_perm, d_pt, nrhs, d_b, ldb,
                                             reinterpret_cast<double*>(ws), s);
     if (!rc) {
-      err = cudaMemcpyAsync(a, d_a, abytes, cudaMemcpyDeviceToHost, s);
+      err = copy_upper(a, d_a, n, lda, cudaMemcpyDeviceToHost, s);
       if (err == cudaSuccess) err = cudaMemcpyAsync(perm, d_perm, n * sizeof(int), cudaMemcpyDeviceToHost, s);
       if (err == cudaSuccess) err = cudaMemcpyAsync(pivot_types, d_pt, n * sizeof(int), cudaMemcpyDeviceToHost, s);
       if (err == cudaSuccess && panel_end)
