@@ -303,7 +303,9 @@ __device__ void exchange(const PanelArgs& P, unsigned tag, unsigned long long ta
 
 // kOrdered: the row and candidate dot products in the reference's order
 // (bitwise the reference); otherwise reassociated (split_dot).
-template <bool kOrdered>
+// kSmemW: the CTA's panel rows live in shared memory (else in global memory,
+// for orders whose slice does not fit).
+template <bool kOrdered, bool kSmemW>
 __global__ void __launch_bounds__(kBlock) panel_kernel(PanelArgs P) {
   extern __shared__ double dsm[];
   __shared__ double s_red_v[kWarps];
@@ -333,12 +335,13 @@ __global__ void __launch_bounds__(kBlock) panel_kernel(PanelArgs P) {
   // (when it fits) the slots' panel rows wsm[m*S + (z - lo)], then the maps
   double* coef = dsm;
   double* wcs = dsm + P.coef_cap;
-  double* wsm = P.w_smem ? wcs + P.smem_cols : nullptr;
+  double* wsm = wcs + P.smem_cols;
   int* win = reinterpret_cast<int*>(
-      wcs + P.smem_cols + (P.w_smem ? static_cast<size_t>(P.win_rows) * P.smem_cols : 0));
+      wcs + P.smem_cols + (kSmemW ? static_cast<size_t>(P.win_rows) * P.smem_cols : 0));
   int* mypos = win + P.win_pad;  // index held by slot lo + zz
   auto wat = [&](int m, int z) -> double& {
-    return wsm ? wsm[m * S + (z - lo)] : P.wslot[m * ldw + z];
+    if (kSmemW) return wsm[m * S + (z - lo)];
+    return P.wslot[m * ldw + z];
   };
   // A(x, z) of the symmetric matrix from its upper triangle (A is not written
   // while the panel runs)
@@ -365,7 +368,7 @@ __global__ void __launch_bounds__(kBlock) panel_kernel(PanelArgs P) {
     const int x = kstart + m, z = lo + zz;
     const double* src = x <= z ? P.a + static_cast<long long>(x) * lda + z
                                : P.a + static_cast<long long>(z) * lda + x;
-    if (wsm)
+    if (kSmemW)
       cp_async_8(&wsm[m * S + zz], src);
     else
       P.wslot[m * ldw + z] = __ldg(src);
@@ -977,9 +980,11 @@ int launch_panel(const FactorPlan& plan, int panel, cudaStream_t s) {
   const size_t limit = 220 * 1024;
   P.w_smem = base + wbytes <= limit;
   const size_t bytes = base + (P.w_smem ? wbytes : 0);
-  const void* fn = plan.mode == BBK_UPDATE_FP64_ORDERED
-                       ? reinterpret_cast<const void*>(panel_kernel<true>)
-                       : reinterpret_cast<const void*>(panel_kernel<false>);
+  const bool ordered = plan.mode == BBK_UPDATE_FP64_ORDERED;
+  const void* fn = ordered ? (P.w_smem ? reinterpret_cast<const void*>(panel_kernel<true, true>)
+                                       : reinterpret_cast<const void*>(panel_kernel<true, false>))
+                           : (P.w_smem ? reinterpret_cast<const void*>(panel_kernel<false, true>)
+                                       : reinterpret_cast<const void*>(panel_kernel<false, false>));
   BBK_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)));
   void* kargs[] = {&P};
   cudaError_t err = cudaLaunchCooperativeKernel(fn, dim3(plan.grid), dim3(kBlock), kargs, bytes, s);
