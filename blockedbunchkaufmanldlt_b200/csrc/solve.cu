@@ -7,10 +7,12 @@
 // L(k+1,k) = 0 when a 2x2 pivot starts at k; D(k,k) = F(k,k) and
 // D(k,k+1) = F(k,k+1) for that 2x2.  With (P A P^T)(i,j) = A(perm[i], perm[j]):
 //   y = B[perm]; L z = y; D w = z; L^T v = w; X[perm] = v.
-// The triangular sweeps are memory-bound: one launch per 64-row block, each
-// CTA solves the block's small triangle redundantly in a warp (one warp per
-// right-hand side, values exchanged by shuffles) and then applies the block's
-// contribution to its own rows, reading every factor entry once per sweep.
+// Each triangular sweep is one persistent cooperative launch over 64-row
+// blocks in wavefront order: CTA c owns blocks c, c+G, ...  A block's owner
+// folds in the contribution of every solved block as soon as its flag is
+// set, solves the block's own triangle (one warp per right-hand side), and
+// publishes it with a release flag.  Only the newest block's contribution and
+// the triangle are on the critical path; the factor is read once per sweep.
 #include <algorithm>
 
 #include "bbk_internal.cuh"
@@ -20,10 +22,7 @@ namespace {
 
 constexpr int kSB = 64;           // solve block
 constexpr int kSolveThreads = 256;
-constexpr int kRowsPerCta = 256;  // forward: rows updated per CTA (one per thread)
-constexpr int kRowsBack = 64;     // backward: rows updated per CTA (warp per row)
 constexpr int kMaxRhsChunk = 8;   // right-hand sides per pass
-constexpr int kKChunk = 16;       // coefficient loads kept in flight per thread
 
 __global__ void gather_kernel(int n, int nrhs, const double* b, long long ldb, const int* perm,
                               double* y) {
@@ -70,129 +69,210 @@ __global__ void dsolve_kernel(int n, int nrhs, const double* f, long long ldf, c
   }
 }
 
-// One block [k0, k1) of the forward (kForward) or backward sweep.  The block's
-// right-hand sides are final in `y` (every earlier block already subtracted
-// its contribution); the solved block goes to `out` (written by CTA 0 only)
-// so no CTA of the launch can read a half-solved block.
-//   forward:  solve L_blk z_blk = y_blk, then y_i -= sum_k F(k,i) z_k for i >= k1
-//   backward: solve L_blk^T v_blk = w_blk, then w_i -= sum_k F(i,k) v_k for i < k0
-template <bool kForward>
-__global__ void __launch_bounds__(kSolveThreads) sweep_kernel(int n, int nrhs, const double* f,
-                                                             long long ldf, const int* pt,
-                                                             double* y, double* out, int k0,
-                                                             int k1) {
-  __shared__ double fs[kSB][kSB + 1];      // fs[r][c] = F(k0 + r, k0 + c), r < c
-  __shared__ double ys[kMaxRhsChunk][kSB];  // solved block values
-  __shared__ int pts[kSB];
-  const int bs = k1 - k0;
-  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  {
-    double v[kSB * kSB / kSolveThreads];
-#pragma unroll
-    for (int it = 0; it < kSB * kSB / kSolveThreads; ++it) {
-      const int idx = t + it * kSolveThreads, r = idx / kSB, c = idx % kSB;
-      v[it] = (r < c && c < bs) ? f[static_cast<long long>(k0 + r) * ldf + k0 + c] : 0.0;
-    }
-#pragma unroll
-    for (int it = 0; it < kSB * kSB / kSolveThreads; ++it) {
-      const int idx = t + it * kSolveThreads;
-      fs[idx / kSB][idx % kSB] = v[it];
-    }
-  }
-  for (int r = t; r < kSB; r += kSolveThreads) pts[r] = r < bs ? pt[k0 + r] : 1;
-  // the 2x2 coupling can straddle the block edge: pivot k0-1 with k0
-  const int pt_before = (k0 > 0) ? pt[k0 - 1] : 1;
-  __syncthreads();
+struct SweepArgs {
+  int n;
+  int nrhs;
+  const double* f;
+  long long ldf;
+  const int* pt;
+  double* y;       // n x nrhs (ld n), solved in place
+  int* flags;      // per block: == mark once the block is solved in this sweep
+  int* status;     // nonzero: a wait ran out; every CTA returns
+  int mark;
+  unsigned long long timeout_ns;
+};
 
-  for (int c0 = 0; c0 < nrhs; c0 += kMaxRhsChunk) {
-    const int nc = min(kMaxRhsChunk, nrhs - c0);
-    // ---- block triangle: one warp per right-hand side
-    for (int cc = warp; cc < nc; cc += kSolveThreads / 32) {
-      const double* yc = y + static_cast<long long>(c0 + cc) * n;
-      double v0 = lane < bs ? yc[k0 + lane] : 0.0;
-      double v1 = lane + 32 < bs ? yc[k0 + lane + 32] : 0.0;
+__device__ __forceinline__ int ld_acquire_s32(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Waits (thread 0, bounded) until block k is solved; all threads learn
+// whether to go on.
+__device__ bool wait_block(const SweepArgs& A, int k, int* s_ok) {
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    const unsigned long long t0 = globaltimer_ns();
+    for (unsigned it = 1; ld_acquire_s32(A.flags + k) != A.mark; ++it) {
+      if ((it & 31u) == 0) {
+        if (ld_relaxed_s32(A.status) != 0) {
+          ok = 0;
+          break;
+        }
+        if (globaltimer_ns() - t0 > A.timeout_ns) {
+          atomicCAS(A.status, 0, BBK_ERR_TIMEOUT);
+          ok = 0;
+          break;
+        }
+      }
+    }
+    *s_ok = ok;
+  }
+  __syncthreads();
+  return *s_ok != 0;
+}
+
+__device__ __forceinline__ void cp_async_8z(double* smem_dst, const double* gsrc, bool valid) {
+  const unsigned saddr = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(saddr), "l"(gsrc), "r"(valid ? 8 : 0)
+               : "memory");
+}
+
+constexpr int kTriPitch = kSB + 1;
+constexpr size_t kSweepSmem = (kSB * kTriPitch + 4 * kMaxRhsChunk * kSB + kMaxRhsChunk * kSB) * sizeof(double);
+
+template <bool kForward>
+__global__ void __launch_bounds__(kSolveThreads) psweep_kernel(SweepArgs A) {
+  extern __shared__ double psm[];
+  double* tri = psm;                               // [kSB][kTriPitch]: F(k0+r, k0+c), r < c
+  double (*red)[kMaxRhsChunk][kSB] =
+      reinterpret_cast<double (*)[kMaxRhsChunk][kSB]>(psm + kSB * kTriPitch);  // 4 quarters
+  double (*zs)[kSB] = reinterpret_cast<double (*)[kSB]>(psm + kSB * kTriPitch + 4 * kMaxRhsChunk * kSB);
+  __shared__ int pts[kSB];
+  __shared__ int s_ok;
+  const int n = A.n, nrhs = A.nrhs;
+  const long long ldf = A.ldf;
+  const int nblk = (n + kSB - 1) / kSB;
+  const int G = gridDim.x, c = blockIdx.x;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const int row = t & (kSB - 1), quarter = t >> 6;  // 64 rows x 4 quarters of the k range
+  const int dir = kForward ? 1 : -1;
+  // this CTA's blocks in wavefront order: first .. last, stride G
+  const int my_first = kForward ? c : (nblk - 1) - ((nblk - 1 - c) % G);
+  if (kForward ? my_first >= nblk : my_first < 0) return;
+  const int my_last = kForward ? c + ((nblk - 1 - c) / G) * G : c;
+  // the diagonal triangle of an own block, streamed into shared memory ahead of time
+  auto prefetch_tri = [&](int b) {
+    const int b0 = b * kSB, bsz = min(n, b0 + kSB) - b0;
+    for (int idx = t; idx < kSB * kSB; idx += kSolveThreads) {
+      const int r = idx / kSB, cc = idx % kSB;
+      const bool ok = r < cc && cc < bsz;
+      cp_async_8z(&tri[r * kTriPitch + cc], ok ? A.f + static_cast<long long>(b0 + r) * ldf + b0 + cc : A.f, ok);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  // factor entries that fold block k into own block b (this thread's 16)
+  auto load_fold = [&](int k, int b, double (&l)[kSB / 4]) {
+    const int k0 = k * kSB, bs = min(n, k0 + kSB) - k0;
+    const int i = b * kSB + row;
+    const int pt_edge = kForward ? A.pt[k0 + bs - 1] : (k0 > 0 ? A.pt[k0 - 1] : 1);
+#pragma unroll
+    for (int u = 0; u < kSB / 4; ++u) {
+      const int kk = quarter * (kSB / 4) + u;
+      const int kg = k0 + kk;
+      bool ok = i < n && kk < bs;
+      double v = 0.0;
       if (kForward) {
-        for (int k = 0; k < bs; ++k) {
-          const double yk = __shfl_sync(0xffffffffu, k < 32 ? v0 : v1, k & 31);
-          const bool skip_next = pts[k] == 2;
-          const int i0 = lane, i1 = lane + 32;
-          if (i0 > k && i0 < bs && !(skip_next && i0 == k + 1)) v0 -= fs[k][i0] * yk;
-          if (i1 > k && i1 < bs && !(skip_next && i1 == k + 1)) v1 -= fs[k][i1] * yk;
-        }
+        // L(i, kg) = F(kg, i); the (kg+1, kg) entry of a 2x2 is zero
+        ok = ok && !(i == kg + 1 && kk == bs - 1 && pt_edge == 2);
+        if (ok) v = A.f[static_cast<long long>(kg) * ldf + i];
       } else {
-        for (int k = bs - 1; k >= 0; --k) {
-          const double yk = __shfl_sync(0xffffffffu, k < 32 ? v0 : v1, k & 31);
-          const int i0 = lane, i1 = lane + 32;
-          // L(k, i) = F(i, k) for i < k, except i == k-1 opening a 2x2
-          if (i0 < k && !(i0 == k - 1 && pts[i0] == 2)) v0 -= fs[i0][k] * yk;
-          if (i1 < k && !(i1 == k - 1 && pts[i1] == 2)) v1 -= fs[i1][k] * yk;
+        // L(kg, i) = F(i, kg); the (i+1, i) entry of a 2x2 is zero
+        ok = ok && !(kg == i + 1 && kk == 0 && pt_edge == 2);
+        if (ok) v = A.f[static_cast<long long>(i) * ldf + kg];
+      }
+      l[u] = v;
+    }
+  };
+  prefetch_tri(my_first);
+  for (int step = 0; step < nblk; ++step) {
+    const int k = kForward ? step : nblk - 1 - step;
+    if (kForward ? k > my_last : k < my_last) break;
+    const int k0 = k * kSB, k1 = min(n, k0 + kSB), bs = k1 - k0;
+    const bool mine = k % G == c;
+    // the nearest own block after k receives k's contribution first (critical path)
+    // (the first b beyond k in wavefront order with b % G == c)
+    const int gap = kForward ? (((c - k) % G) + G) % G : (((k - c) % G) + G) % G;
+    const int near = mine ? k + dir * G : k + dir * gap;
+    const bool has_near = kForward ? near <= my_last : near >= my_last;
+    double lnear[kSB / 4];
+    if (has_near) load_fold(k, near, lnear);
+    if (mine) {
+      // ---- own block: every earlier block's contribution is in; solve the triangle
+      for (int r = t; r < kSB; r += kSolveThreads) pts[r] = r < bs ? A.pt[k0 + r] : 1;
+      asm volatile("cp.async.wait_all;" ::: "memory");
+      __syncthreads();
+      for (int rc = warp; rc < nrhs; rc += kSolveThreads / 32) {
+        double* yc = A.y + static_cast<long long>(rc) * n;
+        double v0 = lane < bs ? yc[k0 + lane] : 0.0;
+        double v1 = lane + 32 < bs ? yc[k0 + lane + 32] : 0.0;
+        if (kForward) {
+          for (int kk = 0; kk < bs; ++kk) {
+            const double yk = __shfl_sync(0xffffffffu, kk < 32 ? v0 : v1, kk & 31);
+            const bool skip_next = pts[kk] == 2;
+            const int i0 = lane, i1 = lane + 32;
+            if (i0 > kk && i0 < bs && !(skip_next && i0 == kk + 1)) v0 -= tri[kk * kTriPitch + i0] * yk;
+            if (i1 > kk && i1 < bs && !(skip_next && i1 == kk + 1)) v1 -= tri[kk * kTriPitch + i1] * yk;
+          }
+        } else {
+          for (int kk = bs - 1; kk >= 0; --kk) {
+            const double yk = __shfl_sync(0xffffffffu, kk < 32 ? v0 : v1, kk & 31);
+            const int i0 = lane, i1 = lane + 32;
+            // L(kk, i) = F(i, kk) for i < kk, except i == kk-1 opening a 2x2
+            if (i0 < kk && !(i0 == kk - 1 && pts[i0] == 2)) v0 -= tri[i0 * kTriPitch + kk] * yk;
+            if (i1 < kk && !(i1 == kk - 1 && pts[i1] == 2)) v1 -= tri[i1 * kTriPitch + kk] * yk;
+          }
         }
+        if (lane < bs) yc[k0 + lane] = v0;
+        if (lane + 32 < bs) yc[k0 + lane + 32] = v1;
       }
-      if (lane < bs) ys[cc][lane] = v0;
-      if (lane + 32 < bs) ys[cc][lane + 32] = v1;
-    }
-    __syncthreads();
-    if (blockIdx.x == 0) {
-      for (int idx = t; idx < nc * bs; idx += kSolveThreads) {
-        const int cc = idx / bs, r = idx % bs;
-        out[static_cast<long long>(c0 + cc) * n + k0 + r] = ys[cc][r];
+      __syncthreads();
+      if (t == 0) {
+        fence_acq_rel_gpu();
+        asm volatile("st.relaxed.gpu.global.b32 [%0], %1;" ::"l"(A.flags + k), "r"(A.mark) : "memory");
       }
+      if (has_near) prefetch_tri(near);  // the triangle buffer is free again
+    } else {
+      if (!wait_block(A, k, &s_ok)) return;
     }
-    // ---- contribution of the block to the other rows
-    if (kForward) {
-      const int i = k1 + blockIdx.x * kRowsPerCta + t;
-      if (i < n) {
+    // ---- fold block k into this CTA's later blocks
+    for (int c0 = 0; c0 < nrhs; c0 += kMaxRhsChunk) {
+      const int nc = min(kMaxRhsChunk, nrhs - c0);
+      __syncthreads();
+      for (int idx = t; idx < nc * kSB; idx += kSolveThreads) {
+        const int cc = idx / kSB, r = idx % kSB;
+        zs[cc][r] = r < bs ? __ldcg(A.y + static_cast<long long>(c0 + cc) * n + k0 + r) : 0.0;
+      }
+      __syncthreads();
+      for (int b = near; has_near && (kForward ? b <= my_last : b >= my_last); b += dir * G) {
+        double lo[kSB / 4];
+        if (b == near) {
+#pragma unroll
+          for (int u = 0; u < kSB / 4; ++u) lo[u] = lnear[u];
+        } else {
+          load_fold(k, b, lo);
+        }
+        const int b0 = b * kSB;
         double acc[kMaxRhsChunk];
 #pragma unroll
         for (int cc = 0; cc < kMaxRhsChunk; ++cc) acc[cc] = 0.0;
-        for (int kc = 0; kc < bs; kc += kKChunk) {
-          double l[kKChunk];
 #pragma unroll
-          for (int kk = 0; kk < kKChunk; ++kk) {
-            const int k = kc + kk;
-            const bool ok = k < bs && !(i == k0 + k + 1 && pts[k] == 2);
-            l[kk] = ok ? f[static_cast<long long>(k0 + k) * ldf + i] : 0.0;
-          }
+        for (int u = 0; u < kSB / 4; ++u)
 #pragma unroll
-          for (int kk = 0; kk < kKChunk; ++kk)
+          for (int cc = 0; cc < kMaxRhsChunk; ++cc)
+            if (cc < nc) acc[cc] += lo[u] * zs[cc][quarter * (kSB / 4) + u];
 #pragma unroll
-            for (int cc = 0; cc < kMaxRhsChunk; ++cc)
-              if (cc < nc && kc + kk < bs) acc[cc] += l[kk] * ys[cc][kc + kk];
-        }
-        for (int cc = 0; cc < nc; ++cc) y[static_cast<long long>(c0 + cc) * n + i] -= acc[cc];
-      }
-    } else {
-      // rows i < k0, F(i, k0..k1) contiguous: one warp per row, four rows per
-      // pass so every lane keeps eight loads in flight
-      const int rows_lo = blockIdx.x * kRowsBack;
-      const int rows_hi = min(k0, rows_lo + kRowsBack);
-      constexpr int kR = 4;
-      for (int i0 = rows_lo + warp * kR; i0 < rows_hi; i0 += kR * (kSolveThreads / 32)) {
-        double l[kR][2];
-#pragma unroll
-        for (int rr = 0; rr < kR; ++rr) {
-          const int i = i0 + rr;
-#pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const int k = lane + 32 * h;
-            const bool ok = i < rows_hi && k < bs && !(k == 0 && i == k0 - 1 && pt_before == 2);
-            l[rr][h] = ok ? f[static_cast<long long>(i) * ldf + k0 + k] : 0.0;
+        for (int cc = 0; cc < kMaxRhsChunk; ++cc)
+          if (cc < nc) red[quarter][cc][row] = acc[cc];
+        __syncthreads();
+        for (int idx = t; idx < nc * kSB; idx += kSolveThreads) {
+          const int cc = idx / kSB, r = idx % kSB;
+          const int ii = b0 + r;
+          if (ii < n) {
+            const double s4 = (red[0][cc][r] + red[1][cc][r]) + (red[2][cc][r] + red[3][cc][r]);
+            A.y[static_cast<long long>(c0 + cc) * n + ii] -= s4;
           }
         }
-        for (int cc = 0; cc < nc; ++cc) {
-          const double y0 = lane < bs ? ys[cc][lane] : 0.0;
-          const double y1 = lane + 32 < bs ? ys[cc][lane + 32] : 0.0;
-#pragma unroll
-          for (int rr = 0; rr < kR; ++rr) {
-            double v = l[rr][0] * y0 + l[rr][1] * y1;
-            for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-            if (lane == 0 && i0 + rr < rows_hi) y[static_cast<long long>(c0 + cc) * n + i0 + rr] -= v;
-          }
-        }
+        __syncthreads();
       }
     }
-    __syncthreads();
   }
+  asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
+__global__ void reset_flags_kernel(int* flags, int count) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) flags[i] = 0;
 }
 
 // M = L D (row-major n x n), M(i,k) for k <= i+1.
@@ -250,32 +330,48 @@ int grid_for(long long work, int threads) {
 
 size_t solve_work_doubles(int n, int nrhs) { return 2 * static_cast<size_t>(n) * nrhs; }
 
-// work: 2 n nrhs doubles (two ping-pong copies of the right-hand sides)
+// work: 2 n nrhs doubles: the right-hand sides being solved in place, then
+// the block flags and the status word.
 int solve_enqueue(int n, const double* f, long long ldf, const int* perm, const int* pivot_types,
                   int nrhs, double* b, long long ldb, double* work, cudaStream_t s) {
   double* y = work;
-  double* z = work + static_cast<size_t>(n) * nrhs;
   const long long total = static_cast<long long>(n) * nrhs;
+  const int nblk = (n + kSB - 1) / kSB;
+  int* flags = reinterpret_cast<int*>(work + total);
+  int* status = flags + nblk;
+  reset_flags_kernel<<<std::max(1, std::min(64, (nblk + 256) / 256)), 256, 0, s>>>(flags, nblk + 1);
+  BBK_CUDA_TRY(cudaGetLastError());
+  count_launch();
   gather_kernel<<<grid_for(total, 256), 256, 0, s>>>(n, nrhs, b, ldb, perm, y);
   BBK_CUDA_TRY(cudaGetLastError());
   count_launch();
-  for (int k0 = 0; k0 < n; k0 += kSB) {
-    const int k1 = std::min(n, k0 + kSB);
-    const int rows = n - k1;
-    const int grid = std::max(1, (rows + kRowsPerCta - 1) / kRowsPerCta);
-    sweep_kernel<true><<<grid, kSolveThreads, 0, s>>>(n, nrhs, f, ldf, pivot_types, y, z, k0, k1);
-    BBK_CUDA_TRY(cudaGetLastError());
+  SweepArgs A{n, nrhs, f, ldf, pivot_types, y, flags, status, 1, wait_timeout_ns()};
+  static bool attr_set[64] = {};
+  int dev = 0;
+  BBK_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64 || !attr_set[dev]) {
+    // 53 KB of dynamic shared memory exceeds the default 48 KB
+    BBK_CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void*>(psweep_kernel<true>),
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSweepSmem)));
+    BBK_CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void*>(psweep_kernel<false>),
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSweepSmem)));
+    if (dev >= 0 && dev < 64) attr_set[dev] = true;
+  }
+  const int grid = std::max(1, std::min(nblk, device_sm_count()));
+  {
+    void* kargs[] = {&A};
+    BBK_CUDA_TRY(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(psweep_kernel<true>), dim3(grid),
+                                             dim3(kSolveThreads), kargs, kSweepSmem, s));
     count_launch();
   }
-  dsolve_kernel<<<grid_for(n, 256), 256, 0, s>>>(n, nrhs, f, ldf, pivot_types, z);
+  dsolve_kernel<<<grid_for(n, 256), 256, 0, s>>>(n, nrhs, f, ldf, pivot_types, y);
   BBK_CUDA_TRY(cudaGetLastError());
   count_launch();
-  const int nblk = (n + kSB - 1) / kSB;
-  for (int bi = nblk - 1; bi >= 0; --bi) {
-    const int k0 = bi * kSB, k1 = std::min(n, k0 + kSB);
-    const int grid = std::max(1, (k0 + kRowsBack - 1) / kRowsBack);
-    sweep_kernel<false><<<grid, kSolveThreads, 0, s>>>(n, nrhs, f, ldf, pivot_types, z, y, k0, k1);
-    BBK_CUDA_TRY(cudaGetLastError());
+  A.mark = 2;
+  {
+    void* kargs[] = {&A};
+    BBK_CUDA_TRY(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(psweep_kernel<false>), dim3(grid),
+                                             dim3(kSolveThreads), kargs, kSweepSmem, s));
     count_launch();
   }
   scatter_kernel<<<grid_for(total, 256), 256, 0, s>>>(n, nrhs, b, ldb, perm, y);
