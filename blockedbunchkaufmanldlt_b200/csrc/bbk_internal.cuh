@@ -155,15 +155,14 @@ struct DeviceState {
 // ---------------------------------------------------------------------------
 // Grid exchange: a grid-wide barrier fused with an all-gather of one small
 // record per CTA.  Each CTA stores its record, then adds one to an arrival
-// counter with release semantics; every CTA polls that single word with
-// acquire loads until all CTAs of this exchange have arrived, and only then
-// reads the records (one pass).  Every record word also carries the
-// exchange's 32-bit tag in its high half, which the reader checks.  Two
-// record sets alternate (tag parity): no CTA can be two exchanges ahead of
-// another.
+// counter; one warp per CTA polls that single word with acquire loads until
+// all CTAs of this exchange have arrived, and then the CTA reads the records
+// (one pass).  Every record word also carries the exchange's 32-bit tag in
+// its high half, which the reader checks.  Two record sets alternate (tag
+// parity): no CTA can be two exchanges ahead of another.
 // ---------------------------------------------------------------------------
-constexpr int kSlotWords = 16;   // words per CTA record
-constexpr int kMaxPub = 6;       // published doubles per record
+constexpr int kSlotWords = 32;   // words per CTA record
+constexpr int kMaxPub = 10;      // published doubles per record
 
 __device__ __forceinline__ unsigned long long tag_word(unsigned tag, unsigned v) {
   return (static_cast<unsigned long long>(tag) << 32) | v;

@@ -691,7 +691,7 @@ static int run_probe(int ctas, int nslots, int iters, unsigned long long timeout
 }
 
 int bbk_probe_bounded_wait(int ctas, unsigned long long timeout_ns, void* stream) {
-  if (ctas <= 0 || ctas > 255 || timeout_ns == 0)
+  if (ctas <= 0 || ctas > 223 || timeout_ns == 0)
     return set_error(BBK_ERR_INVALID_ARGUMENT, "bad probe arguments");
   int rc = check_device();
   if (rc) return rc;
@@ -703,7 +703,7 @@ int bbk_probe_bounded_wait(int ctas, unsigned long long timeout_ns, void* stream
 }
 
 int bbk_probe_exchange_ns(int ctas, int iters, double* ns_per_exchange, void* stream) {
-  if (ctas <= 0 || ctas > 255 || iters <= 0 || !ns_per_exchange)
+  if (ctas <= 0 || ctas > 224 || iters <= 0 || !ns_per_exchange)
     return set_error(BBK_ERR_INVALID_ARGUMENT, "bad probe arguments");
   int rc = check_device();
   if (rc) return rc;

@@ -51,10 +51,12 @@ constexpr int kWarps = kThreads / 32;  // compute warps
 constexpr int kCommWarp = kWarps;       // the communication warp
 constexpr int kBlock = kThreads + 32;   // compute warps + the communication warp
 constexpr int kCols = 3;  // slots per thread: S <= kCols * kThreads
-constexpr int kMaxRecPerLane = 8;  // exchange records read per lane
-constexpr int kMaxGrid = 32 * kMaxRecPerLane;  // CTAs of a panel launch (records per exchange)
-constexpr int kRecBase = 4;  // record words before the published doubles: idx, hi, lo, slot
-static_assert(kRecBase + 2 * kMaxPub <= kSlotWords, "record too large");
+constexpr int kAllWarps = kBlock / 32;
+constexpr int kMaxGrid = kBlock;  // CTAs of a panel launch: every thread reads one record
+constexpr int kRecA = 4;  // argmax words of a record: idx, value hi, value lo, slot
+constexpr int kRecB = 6;  // second argmax: idx, value hi, value lo, slot, payload hi, payload lo
+static_assert(kRecA + kRecB + 2 * kMaxPub <= kSlotWords, "record too large");
+static_assert(kSlotWords <= 32, "one record word per lane of the communication warp");
 
 struct PanelArgs {
   int n;
@@ -86,20 +88,11 @@ struct PanelArgs {
   int nslots;        // records each exchange waits for (gridDim.x normally)
   int slot_stride;   // records per parity in `slots` (>= nslots)
   unsigned long long timeout_ns;
-  int coef_cap;      // doubles reserved for the coefficient column
+  int coef_cap;      // doubles reserved for each coefficient column
   int w_smem;        // keep this CTA's panel rows in shared memory
   int smem_cols;     // slice width the shared-memory allocation holds
   unsigned long long* stats;  // optional per-phase nanoseconds (CTA 0)
-  unsigned long long* pub_ts; // with stats: each CTA's publish timestamp
   unsigned poll_ns;           // pause between polls of the arrival counter
-};
-
-struct ExchangeOut {
-  double val;
-  int idx;
-  int slot;
-  int ok;
-  double pub[kMaxPub];
 };
 
 __device__ __forceinline__ void fail(DeviceState* st, int code) {
@@ -112,17 +105,54 @@ __device__ __forceinline__ double join_hi_lo(unsigned long long hi, unsigned lon
   return __longlong_as_double(static_cast<long long>(bits));
 }
 
+__device__ __forceinline__ unsigned half_of(double x, bool high) {
+  const unsigned long long bits = static_cast<unsigned long long>(__double_as_longlong(x));
+  return high ? static_cast<unsigned>(bits >> 32) : static_cast<unsigned>(bits);
+}
+
+// Argmax candidate of an exchange: value, index, the slot holding the index,
+// and (second channel) a payload double that travels with the winner.
+struct Cand {
+  double v;
+  int i;
+  int s;
+  double pay;
+};
+__device__ __forceinline__ Cand no_cand() { return Cand{0.0, INT_MAX, -1, 0.0}; }
+
 // Argmax combine with the reference's tie rule (src/block_ldlt_decomposition.cc:
 // 164-182 scans ascending columns with a strict '>'): larger value wins, equal
-// values keep the lower index.  The slot travels with its index.  NaN never
-// enters (callers skip it).
-__device__ __forceinline__ void argmax_join(double& v, int& i, int& s, double v2, int i2, int s2) {
-  if (v2 > v || (v2 == v && i2 < i)) {
-    v = v2;
-    i = i2;
-    s = s2;
+// values keep the lower index.  NaN never enters (callers skip it).  With
+// distinct indices this is a total order, so any combine tree gives the same
+// winner.
+__device__ __forceinline__ void argmax_join(Cand& a, const Cand& b) {
+  if (b.v > a.v || (b.v == a.v && b.i < a.i)) a = b;
+}
+
+template <bool kPay>
+__device__ __forceinline__ void warp_argmax(Cand& c) {
+  for (int off = 16; off > 0; off >>= 1) {
+    Cand o;
+    o.v = __shfl_xor_sync(0xffffffffu, c.v, off);
+    o.i = __shfl_xor_sync(0xffffffffu, c.i, off);
+    o.s = __shfl_xor_sync(0xffffffffu, c.s, off);
+    o.pay = kPay ? __shfl_xor_sync(0xffffffffu, c.pay, off) : 0.0;
+    argmax_join(c, o);
   }
 }
+
+// Shared memory of the exchanges.
+struct XShared {
+  Cand pa[kWarps], pb[kWarps];        // this CTA's record: the compute warps' partials
+  Cand ra[kAllWarps], rb[kAllWarps];  // the grid's records: one partial per warp
+  int ok[kAllWarps];
+  double pub[kMaxPub];                // published doubles of this exchange
+};
+
+struct XResult {
+  Cand a, b;
+  bool ok;
+};
 
 __device__ __forceinline__ void cp_async_8(double* smem_dst, const double* gsrc) {
   const unsigned saddr = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
@@ -130,175 +160,166 @@ __device__ __forceinline__ void cp_async_8(double* smem_dst, const double* gsrc)
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-// CTA-collective: reduce (my_val, my_idx, my_slot) over the CTA, publish the
-// CTA's record (reduction + its kMaxPub scalars in pub_in), wait until the
-// arrival counter reaches `target` (all `nslots` CTAs of this exchange), and
-// return the grid-wide argmax plus pub[k] taken from the record of CTA
-// pub_owner[k].  Must be called by every thread.
-__device__ void exchange(const PanelArgs& P, unsigned tag, unsigned long long target, bool release,
-                         double my_val, int my_idx, int my_slot, const double* pub_in,
-                         const int* pub_owner, int npub, double* s_red_v, int* s_red_i, int* s_red_s,
-                         ExchangeOut* out) {
+// CTA-collective grid exchange: reduce this CTA's argmax candidate `ca` (and
+// `cb` with kTwo) over the CTA, publish the CTA's record (the reductions plus
+// the npub doubles of pub_in), and return the grid-wide argmax of every
+// channel once all `nslots` CTAs of this exchange have arrived; X.pub[k] then
+// holds pub_in[k] of CTA pub_owner[k].  Must be called by every thread.
+//
+// Records are structure-of-arrays: word w of CTA c lives at
+// slots[((tag & 1) * kSlotWords + w) * slot_stride + c], so one warp load
+// reads word w of 32 consecutive CTAs.  A CTA stores its record, then adds
+// one to the arrival counter; the communication warp polls that single word
+// (acquire loads) until it reaches `target`, and after a CTA barrier thread
+// c reads the record of CTA c.  Polling the records themselves instead is
+// about three times slower (every SM hammering lines that are being
+// written).  Every record word also carries the exchange's tag in its high
+// half, which the reader checks: the record stores are not ordered before
+// the arrival.  Two record sets alternate (tag parity): no CTA can be two
+// exchanges ahead of another.
+//
+// Ordering.  The arrival is issued by the thread that issued the CTA's
+// release fence (here when `release`, or earlier by the caller, after a CTA
+// barrier that follows the writes to publish), so after the exchange this
+// CTA sees everything the other CTAs wrote before their fence.
+template <bool kTwo>
+__device__ __forceinline__ XResult exchange(const PanelArgs& P, unsigned tag, bool release, Cand ca, Cand cb,
+                                            const double* pub_in, const int (&pub_owner)[kMaxPub], int npub,
+                                            XShared& X) {
+  constexpr int kRec = kRecA + (kTwo ? kRecB : 0);
   const int t = threadIdx.x;
   const int lane = t & 31, warp = t >> 5;
-  for (int off = 16; off > 0; off >>= 1) {
-    const double v2 = __shfl_down_sync(0xffffffffu, my_val, off);
-    const int i2 = __shfl_down_sync(0xffffffffu, my_idx, off);
-    const int s2 = __shfl_down_sync(0xffffffffu, my_slot, off);
-    argmax_join(my_val, my_idx, my_slot, v2, i2, s2);
-  }
+  warp_argmax<false>(ca);
+  if (kTwo) warp_argmax<true>(cb);
   if (lane == 0 && warp < kWarps) {
-    s_red_v[warp] = my_val;
-    s_red_i[warp] = my_idx;
-    s_red_s[warp] = my_slot;
+    X.pa[warp] = ca;
+    if (kTwo) X.pb[warp] = cb;
   }
   __syncthreads();  // also orders this CTA's global writes before a release
-  // Structure-of-arrays records: word w of CTA c lives at
-  // slots[((tag & 1) * kSlotWords + w) * slot_stride + c], so one warp load
-  // reads word w of 32 consecutive CTAs in two cache lines.
   unsigned long long* par_base =
       P.slots + static_cast<size_t>(tag & 1u) * kSlotWords * P.slot_stride;
+  const size_t st = P.slot_stride;
+  const unsigned long long t0 = globaltimer_ns();
   if (warp == kCommWarp) {
-    double v = s_red_v[0];
-    int i = s_red_i[0], sl = s_red_s[0];
-    for (int k = 1; k < kWarps; ++k) argmax_join(v, i, sl, s_red_v[k], s_red_i[k], s_red_s[k]);
-    // one record word per lane: (tag | idx), (tag | hi v), (tag | lo v), (tag | slot), pubs;
-    // the tags tell a reader when each word has landed
-    if (lane < kRecBase + 2 * npub) {
+    Cand a = X.pa[0], b = kTwo ? X.pb[0] : no_cand();
+    for (int k = 1; k < kWarps; ++k) {
+      argmax_join(a, X.pa[k]);
+      if (kTwo) argmax_join(b, X.pb[k]);
+    }
+    if (lane == 0 && release) fence_acq_rel_gpu();
+    if (lane < kRec + 2 * npub) {
       unsigned word;
       if (lane == 0) {
-        word = static_cast<unsigned>(i);
+        word = static_cast<unsigned>(a.i);
+      } else if (lane < 3) {
+        word = half_of(a.v, lane == 1);
       } else if (lane == 3) {
-        word = static_cast<unsigned>(sl);
+        word = static_cast<unsigned>(a.s);
+      } else if (kTwo && lane == 4) {
+        word = static_cast<unsigned>(b.i);
+      } else if (kTwo && lane < 7) {
+        word = half_of(b.v, lane == 5);
+      } else if (kTwo && lane == 7) {
+        word = static_cast<unsigned>(b.s);
+      } else if (kTwo && lane < kRec) {
+        word = half_of(b.pay, lane == 8);
       } else {
-        const double x = lane < 3 ? v : pub_in[(lane - kRecBase) >> 1];
-        const unsigned long long bits = static_cast<unsigned long long>(__double_as_longlong(x));
-        const bool high = lane < 3 ? lane == 1 : ((lane - kRecBase) & 1) == 0;
-        word = high ? static_cast<unsigned>(bits >> 32) : static_cast<unsigned>(bits);
+        word = half_of(pub_in[(lane - kRec) >> 1], ((lane - kRec) & 1) == 0);
       }
-      st_relaxed_u64(par_base + static_cast<size_t>(lane) * P.slot_stride + blockIdx.x,
-                     tag_word(tag, word));
+      st_relaxed_u64(par_base + static_cast<size_t>(lane) * st + blockIdx.x, tag_word(tag, word));
     }
-    // Arrive.  The arrival must release what the CTA wrote for other CTAs
-    // (U columns); the panel issues that fence early, while the compute warps
-    // update the next row, and passes release = false here.
-    if (lane == 0) {
-      if (release) fence_acq_rel_gpu();
-      if (P.pub_ts) P.pub_ts[blockIdx.x] = globaltimer_ns();
-      red_relaxed_add_u64(&P.st->xcount, 1ull);
-    }
-    // Every lane polls the arrival counter (one request per warp load); the
-    // acquire load orders the record reads (and, after the CTA barrier, the
-    // compute warps' reads of U) after it.
-    const unsigned long long t0 = globaltimer_ns();
+    // arrive, then wait for every CTA of this exchange
+    if (lane == 0) red_relaxed_add_u64(&P.st->xcount, 1ull);
+    const unsigned long long target = static_cast<unsigned long long>(P.nslots) * tag;
     bool ok = true;
     for (unsigned iter = 1;; ++iter) {
       if (__all_sync(0xffffffffu, ld_acquire_u64(&P.st->xcount) >= target)) break;
       if (P.poll_ns) __nanosleep(P.poll_ns);
       if ((iter & 31u) == 0) {
-        const bool stop = ld_relaxed_s32(&P.st->abort) != 0;
-        const bool late = globaltimer_ns() - t0 > P.timeout_ns;
-        if (__any_sync(0xffffffffu, stop || late)) {
+        const bool stop = __any_sync(0xffffffffu, ld_relaxed_s32(&P.st->abort) != 0);
+        const bool late = __any_sync(0xffffffffu, globaltimer_ns() - t0 > P.timeout_ns);
+        if (stop || late) {
           if (lane == 0 && !stop) fail(P.st, BBK_ERR_TIMEOUT);
           ok = false;
           break;
         }
       }
     }
-    // Records of CTAs lane, lane+32, ... and this lane's published word pair,
-    // all loads of a pass issued together; a word whose tag is not yet this
-    // exchange's is read again (its store was issued after the arrival).
-    const size_t st = P.slot_stride;
-    double v2 = 0.0;
-    int i2 = INT_MAX, s2 = -1;
-    unsigned long long pw0 = 0, pw1 = 0;
-    const bool has_pub = lane < npub;
-    if (ok) {
-      const int nmine = P.nslots > lane ? (P.nslots - lane + 31) / 32 : 0;  // <= kMaxRecPerLane
-      unsigned long long wv[kMaxRecPerLane][kRecBase];
-      const unsigned long long* psrc =
-          par_base + static_cast<size_t>(kRecBase + 2 * (has_pub ? lane : 0)) * st + (has_pub ? pub_owner[lane] : 0);
-      unsigned pending = (1u << nmine) - 1u;
-      bool pub_pending = has_pub;
-      for (unsigned iter = 1; pending || pub_pending; ++iter) {
-#pragma unroll
-        for (int k = 0; k < kMaxRecPerLane; ++k)
-          if (pending & (1u << k)) {
-            const unsigned long long* src = par_base + lane + 32 * k;
-#pragma unroll
-            for (int w = 0; w < kRecBase; ++w) wv[k][w] = __ldcg(src + w * st);
-          }
-        if (pub_pending) {
-          pw0 = __ldcg(psrc);
-          pw1 = __ldcg(psrc + st);
-        }
-#pragma unroll
-        for (int k = 0; k < kMaxRecPerLane; ++k)
-          if (pending & (1u << k)) {
-            bool all = true;
-#pragma unroll
-            for (int w = 0; w < kRecBase; ++w) all = all && static_cast<unsigned>(wv[k][w] >> 32) == tag;
-            if (all) pending &= ~(1u << k);
-          }
-        if (pub_pending && static_cast<unsigned>(pw0 >> 32) == tag && static_cast<unsigned>(pw1 >> 32) == tag)
-          pub_pending = false;
-        if ((iter & 31u) == 0 && (pending || pub_pending) && globaltimer_ns() - t0 > P.timeout_ns) {
-          fail(P.st, BBK_ERR_TIMEOUT);
-          ok = false;
-          break;
-        }
-      }
-      if (ok) {
-#pragma unroll
-        for (int k = 0; k < kMaxRecPerLane; ++k)
-          if (k < nmine)
-            argmax_join(v2, i2, s2, join_hi_lo(wv[k][1], wv[k][2]), static_cast<int>(wv[k][0] & 0xffffffffu),
-                        static_cast<int>(wv[k][3] & 0xffffffffu));
-      }
-    }
-    for (int off = 16; off > 0; off >>= 1) {
-      const double v3 = __shfl_down_sync(0xffffffffu, v2, off);
-      const int i3 = __shfl_down_sync(0xffffffffu, i2, off);
-      const int s3 = __shfl_down_sync(0xffffffffu, s2, off);
-      argmax_join(v2, i2, s2, v3, i3, s3);
-    }
-    const int all_ok = __all_sync(0xffffffffu, ok);
-    if (P.pub_ts && blockIdx.x == 0 && all_ok) {
-      // diagnostics: (last arrival - own arrival) and (done - last arrival)
-      const unsigned long long done = globaltimer_ns();
-      unsigned long long last = 0;
-      int who = 0;
-      for (int sidx = lane; sidx < P.nslots; sidx += 32) {
-        const unsigned long long lv = __ldcg(P.pub_ts + sidx);
-        if (lv > last) {
-          last = lv;
-          who = sidx;
-        }
-      }
-      for (int off = 16; off > 0; off >>= 1) {
-        const unsigned long long l2 = __shfl_down_sync(0xffffffffu, last, off);
-        const int w2 = __shfl_down_sync(0xffffffffu, who, off);
-        if (l2 > last) {
-          last = l2;
-          who = w2;
-        }
-      }
-      if (lane == 0) {
-        const unsigned long long mine = __ldcg(P.pub_ts);
-        atomicAdd(P.stats + 7, last > mine ? last - mine : 0ull);
-        atomicAdd(P.stats + 8, done > last ? done - last : 0ull);
-        atomicAdd(P.stats + 16 + 1024 + who, 1ull);
-      }
-    }
-    if (has_pub) out->pub[lane] = join_hi_lo(pw0, pw1);
-    if (lane == 0) {
-      out->val = v2;
-      out->idx = i2;
-      out->slot = s2;
-      out->ok = all_ok;
-    }
+    if (lane == 0) X.ok[kAllWarps - 1] = ok;
   }
   __syncthreads();
+  XResult r;
+  r.ok = X.ok[kAllWarps - 1] != 0;
+  if (!r.ok) return r;  // uniform over the CTA
+  // ---- read: thread c reads the record of CTA c; lanes of the communication
+  // warp below npub also read published word pairs.  A word whose tag is not
+  // yet this exchange's is read again (its store may land after the arrival).
+  const bool has_rec = t < P.nslots;
+  const bool has_pub = warp == kCommWarp && lane < npub;
+  int owner = 0;
+#pragma unroll
+  for (int k = 0; k < kMaxPub; ++k)
+    if (lane == k) owner = pub_owner[k];
+  const unsigned long long* rsrc = par_base + (has_rec ? t : 0);
+  const unsigned long long* psrc =
+      par_base + static_cast<size_t>(kRec + 2 * (has_pub ? lane : 0)) * st + (has_pub ? owner : 0);
+  unsigned long long w[kRec];
+  unsigned long long pw0 = 0, pw1 = 0;
+  bool rec_pending = has_rec, pub_pending = has_pub, ok = true;
+  for (unsigned iter = 1;; ++iter) {
+    if (rec_pending) {
+#pragma unroll
+      for (int k = 0; k < kRec; ++k) w[k] = __ldcg(rsrc + k * st);
+    }
+    if (pub_pending) {
+      pw0 = __ldcg(psrc);
+      pw1 = __ldcg(psrc + st);
+    }
+    if (rec_pending) {
+      bool all = true;
+#pragma unroll
+      for (int k = 0; k < kRec; ++k) all = all && static_cast<unsigned>(w[k] >> 32) == tag;
+      rec_pending = !all;
+    }
+    if (pub_pending && static_cast<unsigned>(pw0 >> 32) == tag && static_cast<unsigned>(pw1 >> 32) == tag)
+      pub_pending = false;
+    if (!__any_sync(0xffffffffu, rec_pending || pub_pending)) break;
+    if ((iter & 31u) == 0 && __any_sync(0xffffffffu, globaltimer_ns() - t0 > P.timeout_ns)) {
+      if (lane == 0) fail(P.st, BBK_ERR_TIMEOUT);
+      ok = false;
+      break;
+    }
+  }
+  if (P.stats && blockIdx.x == 0 && t == kThreads) atomicAdd(P.stats + 7, globaltimer_ns() - t0);
+  // ---- reduce the records: per warp, then every thread over the warps
+  Cand ra = no_cand(), rb = no_cand();
+  if (has_rec && ok) {
+    ra = Cand{join_hi_lo(w[1], w[2]), static_cast<int>(w[0] & 0xffffffffu),
+              static_cast<int>(w[3] & 0xffffffffu), 0.0};
+    if (kTwo)
+      rb = Cand{join_hi_lo(w[5], w[6]), static_cast<int>(w[4] & 0xffffffffu),
+                static_cast<int>(w[7] & 0xffffffffu), join_hi_lo(w[8], w[9])};
+  }
+  warp_argmax<false>(ra);
+  if (kTwo) warp_argmax<true>(rb);
+  const int wok = __all_sync(0xffffffffu, ok);
+  if (lane == 0) {
+    X.ra[warp] = ra;
+    if (kTwo) X.rb[warp] = rb;
+    X.ok[warp] = wok;
+  }
+  if (has_pub) X.pub[lane] = join_hi_lo(pw0, pw1);
+  __syncthreads();
+  r.a = X.ra[0];
+  r.b = kTwo ? X.rb[0] : no_cand();
+  r.ok = X.ok[0] != 0;
+#pragma unroll
+  for (int k = 1; k < kAllWarps; ++k) {
+    argmax_join(r.a, X.ra[k]);
+    if (kTwo) argmax_join(r.b, X.rb[k]);
+    r.ok = r.ok && X.ok[k] != 0;
+  }
+  return r;
 }
 
 // kOrdered: the row and candidate dot products in the reference's order
@@ -306,13 +327,10 @@ __device__ void exchange(const PanelArgs& P, unsigned tag, unsigned long long ta
 // kSmemW: the CTA's panel rows live in shared memory (else in global memory,
 // for orders whose slice does not fit).
 template <bool kOrdered, bool kSmemW>
-__global__ void __launch_bounds__(kBlock) panel_kernel(PanelArgs P) {
+__global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
   extern __shared__ double dsm[];
-  __shared__ double s_red_v[kWarps];
-  __shared__ int s_red_i[kWarps];
-  __shared__ int s_red_s[kWarps];
+  __shared__ XShared X;
   __shared__ double s_pub[kMaxPub];
-  __shared__ ExchangeOut s_x;
 
   if (ld_relaxed_s32(&P.st->abort)) return;
   const int G = gridDim.x;
@@ -331,10 +349,11 @@ __global__ void __launch_bounds__(kBlock) panel_kernel(PanelArgs P) {
   const long long lda = P.lda, ldw = P.ldw;
   const int ldu = P.ldu;
   auto owner = [&](int z) -> int { return (z - kstart) / S; };
-  // shared memory: coefficient column, candidate column of this CTA's slots,
+  // shared memory: two coefficient columns, candidate column of this CTA's slots,
   // (when it fits) the slots' panel rows wsm[m*S + (z - lo)], then the maps
   double* coef = dsm;
-  double* wcs = dsm + P.coef_cap;
+  double* coef2 = dsm + P.coef_cap;  // coefficients of a row computed ahead
+  double* wcs = dsm + 2 * P.coef_cap;
   double* wsm = wcs + P.smem_cols;
   int* win = reinterpret_cast<int*>(
       wcs + P.smem_cols + (kSmemW ? static_cast<size_t>(P.win_rows) * P.smem_cols : 0));
@@ -377,106 +396,128 @@ __global__ void __launch_bounds__(kBlock) panel_kernel(PanelArgs P) {
   __syncthreads();
 
   // exchanges are numbered across the factorization; the k-th (from 1) uses
-  // tag k and completes when the arrival counter reaches nslots * k
+  // tag k
   unsigned seq = static_cast<unsigned>(ldcg(&P.st->xseq[P.panel & 1]));
-  const unsigned long long nslots64 = static_cast<unsigned long long>(P.nslots);
   int p = kstart;
   // coefficients U[q, p] of the current row: rows q < n_old from the Uslot
   // column of p's slot, then lp - n_old (<= 2) values computed by every CTA.
   int n_old = 0;
   double extra0 = 0.0, extra1 = 0.0;
-  int ncand = 0;
+  int ncand = 0, nahead = 0;
   // the next row's coefficient column, loaded during the scaling phase when
   // it has at most 2 * kThreads rows
   double cpre[2] = {0.0, 0.0};
   bool coef_pre = false;
+  // Rows computed ahead.  A candidate step whose outcome may be "keep the
+  // 1x1 pivot p" (r != p+1) also updates row p+1 during its candidate phase,
+  // as that outcome would leave it, and reduces that row's argmax in the
+  // candidate exchange.  When the pivot is kept, the next step starts with
+  // its row and argmax known and skips its row update and first exchange.
+  // Its U row (written by this step's scaling, after the last exchange) is
+  // then not yet visible to other CTAs: the two values of that row the next
+  // step needs travel as scalars (u_prev_r = U[p, r'] for its candidate
+  // column, carry = U[p, p+2] for the row after it), and its candidate phase
+  // releases the row.  In the ordered mode row p+1 is summed in the
+  // reference's order (the last term, which involves the candidate's result
+  // at column r, is added after the exchange), so results do not change.
+  bool ahead = false;
+  double nx_omega = 0.0, nx_dpp = 0.0, nx_w1 = 0.0, nx_w2 = 0.0;
+  int nx_r = 0, nx_rs = 0;
+  double u_prev_r = 0.0, carry = 0.0;
 
   while (p < P.nominal_end) {
     const int lp = p - kstart;
     const int sp = win[lp];
-    // the row of p is staged in shared memory unless an interchange gave p a
-    // slot whose staged row was already consumed
-    const bool staged = (sp - kstart) == lp;
-    // ---- row update: W[p, j] = A[p, j] - sum_q U[q, p] W[q, j]
-    // (CopyCurrentRowToWorkspace + UpdateCurrentRowInWorkspace, :122-162)
-    double av[kCols];
+    const bool was_ahead = ahead;
+    ahead = false;
+    // U rows whose writes by other CTAs this CTA may read: every row before
+    // lp, except the previous one when this row was computed ahead
+    const int nrel = was_ahead ? lp - 1 : lp;
+    double omega, dpp, w_p1, w_p2;
+    int r, rs;
+    if (!was_ahead) {
+      // the row of p is staged in shared memory unless an interchange gave p a
+      // slot whose staged row was already consumed
+      const bool staged = (sp - kstart) == lp;
+      // ---- row update: W[p, j] = A[p, j] - sum_q U[q, p] W[q, j]
+      // (CopyCurrentRowToWorkspace + UpdateCurrentRowInWorkspace, :122-162)
+      double av[kCols];
 #pragma unroll
-    for (int k = 0; k < kCols; ++k) {
-      const int z = lo + tz + k * kThreads;
-      double v = 0.0;
-      if (z < hi && mypos[z - lo] >= p) v = staged ? wat(lp, z) : asym(sp, z);
-      av[k] = v;
-    }
-    {
-      if (coef_pre) {
-        if (tz < n_old) coef[tz] = cpre[0];
-        if (tz + kThreads < n_old) coef[tz + kThreads] = cpre[1];
-      } else {
-        const double* ucol = P.uslot + static_cast<size_t>(sp) * ldu;
-        for (int q = t; q < n_old; q += kBlock) coef[q] = ldcg(ucol + q);
+      for (int k = 0; k < kCols; ++k) {
+        const int z = lo + tz + k * kThreads;
+        double v = 0.0;
+        if (z < hi && mypos[z - lo] >= p) v = staged ? wat(lp, z) : asym(sp, z);
+        av[k] = v;
       }
-      if (t == 0) {
-        coef[n_old] = extra0;
-        coef[n_old + 1] = extra1;
+      {
+        if (coef_pre) {
+          if (tz < n_old) coef[tz] = cpre[0];
+          if (tz + kThreads < n_old) coef[tz + kThreads] = cpre[1];
+        } else {
+          const double* ucol = P.uslot + static_cast<size_t>(sp) * ldu;
+          for (int q = t; q < n_old; q += kBlock) coef[q] = ldcg(ucol + q);
+        }
+        if (t == 0) {
+          coef[n_old] = extra0;
+          coef[n_old + 1] = extra1;
+        }
+        if (t < kMaxPub) s_pub[t] = 0.0;
       }
-      if (t < kMaxPub) s_pub[t] = 0.0;
-    }
-    __syncthreads();
-    // release the previous step's U columns while the compute warps update the row
-    if (t == kThreads) fence_acq_rel_gpu();
-    double best = 0.0;
-    int best_j = INT_MAX, best_z = -1;
+      __syncthreads();
+      // release the previous steps' U rows while the compute warps update the row
+      if (t == kThreads) fence_acq_rel_gpu();
+      Cand best = no_cand();
 #pragma unroll
-    for (int k = 0; k < kCols; ++k) {
-      const int z = lo + tz + k * kThreads;
-      if (z < hi) {
-        const int j = mypos[z - lo];
-        if (j >= p) {
-          const double acc = kOrdered ? ordered_dot(coef, lp, [&](int q) { return wat(q, z); })
-                                      : split_dot(coef, lp, [&](int q) { return wat(q, z); });
-          const double wv = xsub(av[k], acc);
-          wat(lp, z) = wv;
-          if (j > p) {
-            const double v = fabs(wv);
-            if (v > best || (v == best && j < best_j)) {  // FindCurrentRowMax, :164-182
-              best = v;
-              best_j = j;
-              best_z = z;
-            }
-          } else {
-            s_pub[0] = wv;  // W[p, p]
+      for (int k = 0; k < kCols; ++k) {
+        const int z = lo + tz + k * kThreads;
+        if (z < hi) {
+          const int j = mypos[z - lo];
+          if (j >= p) {
+            const double acc = kOrdered ? ordered_dot(coef, lp, [&](int q) { return wat(q, z); })
+                                        : split_dot(coef, lp, [&](int q) { return wat(q, z); });
+            const double wv = xsub(av[k], acc);
+            wat(lp, z) = wv;
+            if (j > p)
+              argmax_join(best, Cand{fabs(wv), j, z, 0.0});  // FindCurrentRowMax, :164-182
+            else
+              s_pub[0] = wv;  // W[p, p]
+            if (j == p + 1) s_pub[1] = wv;
+            if (j == p + 2) s_pub[2] = wv;
           }
-          if (j == p + 1) s_pub[1] = wv;
-          if (j == p + 2) s_pub[2] = wv;
         }
       }
+      lap(0);
+      int owners[kMaxPub] = {};
+      owners[0] = owner(sp);
+      owners[1] = lp + 1 < nwin ? owner(win[lp + 1]) : 0;
+      owners[2] = lp + 2 < nwin ? owner(win[lp + 2]) : 0;
+      const XResult x1 = exchange<false>(P, ++seq, false, best, no_cand(), s_pub, owners, 3, X);
+      if (!x1.ok) return;
+      omega = x1.a.v;
+      r = x1.a.i;
+      rs = x1.a.s;  // slot of r
+      dpp = X.pub[0];
+      w_p1 = X.pub[1];  // W[p, p+1] (current-row version)
+      w_p2 = X.pub[2];  // W[p, p+2]
+    } else {
+      ++nahead;
+      omega = nx_omega;
+      r = nx_r;
+      rs = nx_rs;
+      dpp = nx_dpp;
+      w_p1 = nx_w1;
+      w_p2 = nx_w2;
     }
-    lap(0);
-    int owners[kMaxPub];
-    owners[0] = owner(sp);
-    owners[1] = lp + 1 < nwin ? owner(win[lp + 1]) : 0;
-    owners[2] = lp + 2 < nwin ? owner(win[lp + 2]) : 0;
-    const unsigned x1 = ++seq;
-    exchange(P, x1, nslots64 * x1, false, best, best_j, best_z, s_pub, owners, 3, s_red_v, s_red_i,
-             s_red_s, &s_x);
-    if (!s_x.ok) return;
-    const double omega = s_x.val;
-    const int r = s_x.idx;
-    const int rs = s_x.slot;  // slot of r
-    const double dpp = s_x.pub[0];
-    const double w_p1 = s_x.pub[1];  // W[p, p+1] (current-row version)
-    const double w_p2 = s_x.pub[2];  // W[p, p+2]
-    __syncthreads();
     lap(1);
-    // The next row's coefficient column (rows q < lp, written before this
-    // step and visible since this exchange) is loaded now for every slot the
-    // next row may have, so its latency hides behind the rest of the step:
-    // A = slot of p+1, B = slot of p+2 (2x2 pivot), C = slot of p (r = p+1).
+    // The next row's coefficient column (the visible rows q < nrel) is loaded
+    // now for every slot the next row may have, so its latency hides behind
+    // the rest of the step: A = slot of p+1, B = slot of p+2 (2x2 pivot),
+    // C = slot of p (r = p+1).
     const bool prefetch = lp <= 2 * kThreads;
     auto preload = [&](int slot, double& c0, double& c1) {
       const double* ucol = P.uslot + static_cast<size_t>(slot) * ldu;
-      c0 = tz < lp ? ldcg(ucol + tz) : 0.0;
-      c1 = tz + kThreads < lp ? ldcg(ucol + tz + kThreads) : 0.0;
+      c0 = tz < nrel ? ldcg(ucol + tz) : 0.0;
+      c1 = tz + kThreads < nrel ? ldcg(ucol + tz + kThreads) : 0.0;
     };
     const int slot_a = lp + 1 < nwin ? win[lp + 1] : -1;
     int slot_b = -1, slot_c = -1;
@@ -484,8 +525,11 @@ __global__ void __launch_bounds__(kBlock) panel_kernel(PanelArgs P) {
     if (prefetch && slot_a >= 0) preload(slot_a, ca0, ca1);
 
     int kind = 1;  // 1: 1x1 at p; -1: 1x1 after p<->r; 2: 2x2 with p+1<->r
-    bool cand = false;
+    bool cand = false, spec = false;
     double wc_r = 0.0, wc_p = 0.0, wc_p1 = 0.0, wc_p2 = 0.0;
+    double sv[kCols] = {};  // row p+1 computed ahead (columns other than r)
+    double nx_ar = 0.0, nx_part = 0.0, nx_d = 0.0, nx_1 = 0.0, nx_2 = 0.0;
+    Cand nx_best = no_cand();
     // FactorPanel's test, :90-92
     if (!(fabs(dpp) >= xmul(kAlpha, omega) || omega == 0.0)) {
       cand = true;
@@ -494,6 +538,7 @@ __global__ void __launch_bounds__(kBlock) panel_kernel(PanelArgs P) {
       slot_c = r == p + 1 ? sp : -1;
       if (prefetch && slot_b >= 0) preload(slot_b, cb0, cb1);
       if (prefetch && slot_c >= 0) preload(slot_c, cc0, cc1);
+      spec = r != p + 1 && p + 1 < P.nominal_end && slot_a >= 0;
       // ---- candidate column W(i, r) = A(i, r) - sum_q U[q, r] W[q, i]
       // (CopyCandidateToWorkspace + UpdateCandidateInWorkspace, :184-352)
       double cv[kCols];
@@ -502,12 +547,75 @@ __global__ void __launch_bounds__(kBlock) panel_kernel(PanelArgs P) {
         const int z = lo + tz + k * kThreads;
         cv[k] = (z < hi && mypos[z - lo] >= p) ? asym(z, rs) : 0.0;
       }
-      {
-        const double* ucol = P.uslot + static_cast<size_t>(rs) * ldu;
-        for (int q = t; q < lp; q += kBlock) coef[q] = ldcg(ucol + q);
-        if (t < kMaxPub) s_pub[t] = 0.0;
+      double cr0 = 0.0, cr1 = 0.0;
+      if (prefetch) preload(rs, cr0, cr1);
+      // the candidate's coefficients U[q, r]: the visible rows from r's slot,
+      // then U[lp - 1, r] passed along by the previous step
+      auto put_cand_coef = [&]() {
+        if (prefetch) {
+          if (tz < nrel) coef[tz] = cr0;
+          if (tz + kThreads < nrel) coef[tz + kThreads] = cr1;
+        } else {
+          const double* ucol = P.uslot + static_cast<size_t>(rs) * ldu;
+          for (int q = t; q < nrel; q += kBlock) coef[q] = ldcg(ucol + q);
+        }
+        if (was_ahead && t == 0) coef[lp - 1] = u_prev_r;
+      };
+      if (spec) {
+        // row p+1's coefficients U[q, p+1] for q < lp (U[lp, p+1] is applied last)
+        if (prefetch) {
+          if (tz < nrel) coef2[tz] = ca0;
+          if (tz + kThreads < nrel) coef2[tz + kThreads] = ca1;
+        } else {
+          const double* ucol = P.uslot + static_cast<size_t>(slot_a) * ldu;
+          for (int q = t; q < nrel; q += kBlock) coef2[q] = ldcg(ucol + q);
+        }
+        if (was_ahead && t == 0) coef2[lp - 1] = carry;
+      } else {
+        put_cand_coef();
       }
+      if (t < kMaxPub) s_pub[t] = 0.0;
       __syncthreads();
+      // release U row lp - 1 (written by the previous step, after its last exchange)
+      if (was_ahead && t == kThreads) fence_acq_rel_gpu();
+      if (spec) {
+        // ---- row p+1 as keeping pivot p leaves it: W[p+1, j] = A(p+1, j) -
+        // (sum_{q < lp} U[q, p+1] W[q, j] + U[lp, p+1] W[lp, j]); at j = r,
+        // W[lp, r] becomes the candidate's W(p, r), so the owner publishes
+        // A(p+1, r) and the partial sum instead
+        const bool staged1 = (slot_a - kstart) == lp + 1;
+        const double e0 = div_or_zero(w_p1, safe_denominator(dpp));
+        Cand best = no_cand();
+#pragma unroll
+        for (int k = 0; k < kCols; ++k) {
+          const int z = lo + tz + k * kThreads;
+          if (z < hi) {
+            const int j = mypos[z - lo];
+            if (j > p) {
+              const double a1 = staged1 ? wat(lp + 1, z) : asym(slot_a, z);
+              const double part = kOrdered ? ordered_dot(coef2, lp, [&](int q) { return wat(q, z); })
+                                           : split_dot(coef2, lp, [&](int q) { return wat(q, z); });
+              if (j != r) {
+                const double wp = wat(lp, z);
+                const double v1 = xsub(a1, xadd(part, xmul(e0, wp)));
+                sv[k] = v1;
+                if (j > p + 1)
+                  argmax_join(best, Cand{fabs(v1), j, z, wp});
+                else
+                  s_pub[4] = v1;  // W[p+1, p+1]
+                if (j == p + 2) s_pub[5] = v1;
+                if (j == p + 3) s_pub[6] = v1;
+              } else {
+                s_pub[7] = a1;
+                s_pub[8] = part;
+              }
+            }
+          }
+        }
+        nx_best = best;
+        put_cand_coef();
+        __syncthreads();
+      }
       double sig = 0.0;
 #pragma unroll
       for (int k = 0; k < kCols; ++k) {
@@ -532,20 +640,34 @@ __global__ void __launch_bounds__(kBlock) panel_kernel(PanelArgs P) {
         }
       }
       lap(2);
+      int owners[kMaxPub] = {};
       owners[0] = owner(rs);
       owners[1] = owner(sp);
       owners[2] = lp + 1 < nwin ? owner(win[lp + 1]) : 0;
       owners[3] = lp + 2 < nwin ? owner(win[lp + 2]) : 0;
-      const unsigned x2 = ++seq;
-      exchange(P, x2, nslots64 * x2, false, sig, 0, 0, s_pub, owners, 4, s_red_v, s_red_i, s_red_s,
-               &s_x);
-      if (!s_x.ok) return;
-      const double sigma = s_x.val;
-      wc_r = s_x.pub[0];
-      wc_p = s_x.pub[1];
-      wc_p1 = s_x.pub[2];
-      wc_p2 = s_x.pub[3];
-      __syncthreads();
+      if (spec) {
+        owners[4] = owner(slot_a);
+        owners[5] = owners[3];
+        owners[6] = lp + 3 < nwin ? owner(win[lp + 3]) : 0;
+        owners[7] = owners[0];
+        owners[8] = owners[0];
+      }
+      const XResult x2 = exchange<true>(P, ++seq, false, Cand{sig, 0, 0, 0.0}, nx_best, s_pub, owners,
+                                        spec ? 9 : 4, X);
+      if (!x2.ok) return;
+      const double sigma = x2.a.v;
+      wc_r = X.pub[0];
+      wc_p = X.pub[1];
+      wc_p1 = X.pub[2];
+      wc_p2 = X.pub[3];
+      if (spec) {
+        nx_best = x2.b;
+        nx_d = X.pub[4];
+        nx_1 = X.pub[5];
+        nx_2 = X.pub[6];
+        nx_ar = X.pub[7];
+        nx_part = X.pub[8];
+      }
       lap(3);
       // SelectPivot, :369-390
       if (xsub(xmul(fabs(dpp), sigma), xmul(xmul(kAlpha, omega), omega)) >= 0.0) {
@@ -565,6 +687,8 @@ __global__ void __launch_bounds__(kBlock) panel_kernel(PanelArgs P) {
       // reference's W(p, r) holds the column version of that entry.
       const double d = dpp;
       const double den = safe_denominator(d);
+      double wr = 0.0;  // W[p+1, r] of the row computed ahead
+      if (spec) wr = xsub(nx_ar, xadd(nx_part, xmul(div_or_zero(w_p1, den), wc_p)));
 #pragma unroll
       for (int k = 0; k < kCols; ++k) {
         const int z = lo + tz + k * kThreads;
@@ -579,6 +703,7 @@ __global__ void __launch_bounds__(kBlock) panel_kernel(PanelArgs P) {
               wv = wat(lp, z);
             }
             P.uslot[static_cast<size_t>(z) * ldu + lp] = div_or_zero(wv, den);
+            if (spec) wat(lp + 1, z) = j == r ? wr : sv[k];
           }
         }
       }
@@ -586,9 +711,31 @@ __global__ void __launch_bounds__(kBlock) panel_kernel(PanelArgs P) {
         P.dlog[2 * lp] = d;
         P.ptype[p] = 1;
       }
-      // next row's coefficients: U[q, p+1] for q < p, then U[p, p+1]
-      n_old = lp;
-      extra0 = div_or_zero((cand && r == p + 1) ? wc_p : w_p1, den);
+      if (spec) {
+        // the next step starts from row p+1 and its argmax
+        Cand best = nx_best;
+        argmax_join(best, Cand{fabs(wr), r, rs, wc_p});
+        nx_omega = best.v;
+        nx_r = best.i;
+        nx_rs = best.s;
+        nx_dpp = nx_d;
+        nx_w1 = r == p + 2 ? wr : nx_1;
+        nx_w2 = r == p + 3 ? wr : nx_2;
+        u_prev_r = div_or_zero(best.pay, den);
+        carry = div_or_zero(r == p + 2 ? wc_p : w_p2, den);
+        ahead = true;
+      }
+      if (was_ahead && !cand) {
+        // next row's coefficients: U[q, p+1] for q < lp - 1, then U[lp - 1, p+1]
+        // (passed along) and U[p, p+1]
+        n_old = lp - 1;
+        extra0 = carry;
+        extra1 = div_or_zero(w_p1, den);
+      } else {
+        // next row's coefficients: U[q, p+1] for q < p, then U[p, p+1]
+        n_old = lp;
+        extra0 = div_or_zero((cand && r == p + 1) ? wc_p : w_p1, den);
+      }
       p += 1;
     } else if (kind == -1) {
       // SwapOneByOnePivot (:392-401, :414-498) + ScaleOneByOnePivot: p and r
@@ -662,7 +809,7 @@ __global__ void __launch_bounds__(kBlock) panel_kernel(PanelArgs P) {
       extra1 = xadd(xmul(i21, x), xmul(i22, y));
       p += 2;
     }
-    coef_pre = prefetch && p < P.nominal_end;
+    coef_pre = prefetch && p < P.nominal_end && !ahead;
     if (coef_pre) {
       const int next = win[p - kstart];
       if (next == slot_a) {
@@ -676,6 +823,12 @@ __global__ void __launch_bounds__(kBlock) panel_kernel(PanelArgs P) {
         cpre[1] = cc1;
       } else {
         preload(next, cpre[0], cpre[1]);
+      }
+      // U row nrel, released by this step's candidate exchange
+      if (n_old > nrel) {
+        const double* ucol = P.uslot + static_cast<size_t>(next) * ldu;
+        if (tz == nrel) cpre[0] = ldcg(ucol + nrel);
+        if (tz + kThreads == nrel) cpre[1] = ldcg(ucol + nrel);
       }
     }
     __syncthreads();
@@ -715,14 +868,14 @@ __global__ void __launch_bounds__(kBlock) panel_kernel(PanelArgs P) {
       for (int k = 0; k < 5; ++k) atomicAdd(P.stats + k, tm[k]);
       atomicAdd(P.stats + 5, static_cast<unsigned long long>(kb));
       atomicAdd(P.stats + 6, static_cast<unsigned long long>(ncand));
+      atomicAdd(P.stats + 9, static_cast<unsigned long long>(nahead));
     }
   }
   // grid barrier: every CTA's maps and lists are visible after it
   {
-    int owners0[kMaxPub] = {0, 0, 0, 0, 0, 0};
-    const unsigned xb = ++seq;
-    exchange(P, xb, nslots64 * xb, true, 0.0, 0, 0, s_pub, owners0, 0, s_red_v, s_red_i, s_red_s, &s_x);
-    if (!s_x.ok) return;
+    const int owners0[kMaxPub] = {};
+    const XResult xb = exchange<false>(P, ++seq, true, no_cand(), no_cand(), s_pub, owners0, 0, X);
+    if (!xb.ok) return;
   }
   // ---- gather the interchanged data (written back by finalize_kernel)
   const int cnt = ldcg(&P.st->moved[P.panel & 1]);
@@ -872,20 +1025,17 @@ __global__ void status_copy_kernel(const DeviceState* st, int* out) {
 // back to back and CTA 0 stores the elapsed nanoseconds in stats[0] (the
 // exchange-latency measurement).
 __global__ void __launch_bounds__(kBlock) probe_kernel(PanelArgs P) {
-  __shared__ double s_red_v[kWarps];
-  __shared__ int s_red_i[kWarps];
-  __shared__ int s_red_s[kWarps];
+  __shared__ XShared X;
   __shared__ double s_pub[kMaxPub];
-  __shared__ ExchangeOut s_x;
   if (threadIdx.x < kMaxPub) s_pub[threadIdx.x] = 0.0;
-  int owners[kMaxPub] = {0, 0, 0, 0, 0, 0};
+  const int owners[kMaxPub] = {};
   __syncthreads();
   const unsigned long long t0 = globaltimer_ns();
   for (int it = 0; it < P.n; ++it) {
-    const unsigned x = static_cast<unsigned>(it) + 1u;
-    exchange(P, x, static_cast<unsigned long long>(P.nslots) * x, true, static_cast<double>(blockIdx.x),
-             blockIdx.x, blockIdx.x, s_pub, owners, 3, s_red_v, s_red_i, s_red_s, &s_x);
-    if (!s_x.ok) return;
+    const Cand mine{static_cast<double>(blockIdx.x), static_cast<int>(blockIdx.x), static_cast<int>(blockIdx.x), 0.0};
+    const XResult x = exchange<false>(P, static_cast<unsigned>(it) + 1u, true, mine, no_cand(), s_pub,
+                                      owners, 3, X);
+    if (!x.ok) return;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0 && P.stats) P.stats[0] = globaltimer_ns() - t0;
 }
@@ -961,7 +1111,6 @@ int launch_panel(const FactorPlan& plan, int panel, cudaStream_t s) {
   P.slot_stride = plan.grid;
   P.timeout_ns = plan.timeout_ns;
   P.stats = plan.stats;
-  P.pub_ts = plan.stats ? plan.stats + 16 : nullptr;
   static const unsigned poll_ns = [] {
     const char* e = getenv("BBK_POLL_NS");
     return e ? static_cast<unsigned>(atoi(e)) : 0u;
@@ -969,12 +1118,12 @@ int launch_panel(const FactorPlan& plan, int panel, cudaStream_t s) {
   P.poll_ns = poll_ns;
   if (plan.grid > kMaxGrid)
     return set_error(BBK_ERR_INVALID_ARGUMENT, "panel grid %d exceeds %d", plan.grid, kMaxGrid);
-  // shared memory: coefficient column + candidate column + (if it fits) the
+  // shared memory: two coefficient columns + candidate column + (if it fits) the
   // slots' panel rows, then the window map and the slot -> index map
   const int smax = (plan.n + plan.grid - 1) / plan.grid;
   P.coef_cap = static_cast<int>(align_up(static_cast<size_t>(plan.b) + 4, 2));
   P.smem_cols = smax;
-  const size_t base = (static_cast<size_t>(P.coef_cap) + smax) * sizeof(double) +
+  const size_t base = (2 * static_cast<size_t>(P.coef_cap) + smax) * sizeof(double) +
                       (static_cast<size_t>(P.win_pad) + smax) * sizeof(int);
   const size_t wbytes = static_cast<size_t>(P.win_rows) * smax * sizeof(double);
   const size_t limit = 220 * 1024;
@@ -1028,6 +1177,8 @@ int launch_status_copy(const DeviceState* st, int* status_out, cudaStream_t s) {
 int launch_probe_wait(int ctas, int nslots, int iters, unsigned long long timeout_ns,
                       DeviceState* st, unsigned long long* slots, unsigned long long* stats,
                       cudaStream_t s) {
+  if (nslots > kMaxGrid + 1 || ctas > kMaxGrid)
+    return set_error(BBK_ERR_INVALID_ARGUMENT, "probe: %d blocks exceed %d", ctas, kMaxGrid);
   PanelArgs P{};
   P.slots = slots;
   P.st = st;

@@ -77,12 +77,12 @@ unsigned long long bbk_kernel_launch_count(void);
  * BBK_ERR_TIMEOUT instead of hanging.  Default 5 s. */
 int bbk_set_wait_timeout_ns(unsigned long long timeout_ns);
 /* Test hook for the bounded-wait machinery: launches one cooperative grid of
- * `ctas` (1..255) blocks whose exchange also waits for one participant that
+ * `ctas` (1..223) blocks whose exchange also waits for one participant that
  * does not exist, so the wait must run out.  Returns BBK_ERR_TIMEOUT when the bound
  * works (and leaves the context usable), BBK_OK never. */
 int bbk_probe_bounded_wait(int ctas, unsigned long long timeout_ns, void* stream);
 /* Diagnostics: runs `iters` back-to-back grid exchanges (the panel kernel's
- * barrier + all-gather) on `ctas` (1..255) co-resident blocks and reports the
+ * barrier + all-gather) on `ctas` (1..224) co-resident blocks and reports the
  * mean device nanoseconds per exchange. */
 int bbk_probe_exchange_ns(int ctas, int iters, double* ns_per_exchange, void* stream);
 
