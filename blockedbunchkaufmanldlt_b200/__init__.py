@@ -198,8 +198,8 @@ def panel_stats(enable: bool):
     d = {k: out[i] / 1e6 for i, k in enumerate(PANEL_PHASES)}  # ms
     d["pivots"] = int(out[5])
     d["candidates"] = int(out[6])
-    d["exchange_wait_for_last_ms"] = out[7] / 1e6
-    d["exchange_propagation_ms"] = out[8] / 1e6
+    d["exchange_ms"] = out[7] / 1e6  # CTA 0: from its arrival to the records read, all exchanges
+    d["rows_ahead"] = int(out[9])  # steps whose row the previous candidate phase computed
     return d
 
 

@@ -122,6 +122,62 @@ __device__ __forceinline__ double ordered_dot(const double* c, int count, WGet&&
   return acc;
 }
 
+// Two sums over the same w(q) at once: s1 = sum c1[q] w(q), s2 = sum c2[q] w(q),
+// each added in ascending q with every product and sum rounded separately,
+// so each is bitwise ordered_dot of its coefficients; w(q) is read once.
+template <typename WGet>
+__device__ __forceinline__ void ordered_dot2(const double* c1, const double* c2, int count, WGet&& w,
+                                             double& s1, double& s2) {
+  double a1 = 0.0, a2 = 0.0;
+  int q = 0;
+  for (; q + 4 <= count; q += 4) {
+    double p1[4], p2[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const double x = w(q + u);
+      p1[u] = xmul(c1[q + u], x);
+      p2[u] = xmul(c2[q + u], x);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      a1 = xadd(a1, p1[u]);
+      a2 = xadd(a2, p2[u]);
+    }
+  }
+  for (; q < count; ++q) {
+    const double x = w(q);
+    a1 = xadd(a1, xmul(c1[q], x));
+    a2 = xadd(a2, xmul(c2[q], x));
+  }
+  s1 = a1;
+  s2 = a2;
+}
+
+// The reassociated counterpart of ordered_dot2: four FMA accumulators per sum.
+template <typename WGet>
+__device__ __forceinline__ void split_dot2(const double* c1, const double* c2, int count, WGet&& w,
+                                           double& s1, double& s2) {
+  double a[4] = {0.0, 0.0, 0.0, 0.0}, b[4] = {0.0, 0.0, 0.0, 0.0};
+  int q = 0;
+  for (; q + 4 <= count; q += 4) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const double x = w(q + u);
+      a[u] = __fma_rn(c1[q + u], x, a[u]);
+      b[u] = __fma_rn(c2[q + u], x, b[u]);
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+    if (q + u < count) {
+      const double x = w(q + u);
+      a[u] = __fma_rn(c1[q + u], x, a[u]);
+      b[u] = __fma_rn(c2[q + u], x, b[u]);
+    }
+  s1 = (a[0] + a[1]) + (a[2] + a[3]);
+  s2 = (b[0] + b[1]) + (b[2] + b[3]);
+}
+
 // sum_{q < count} c[q] * w(q) with eight independent FMA accumulators
 // combined pairwise: the same sum, reassociated, with an eighth of the
 // dependent-latency chain (update modes that do not reproduce the

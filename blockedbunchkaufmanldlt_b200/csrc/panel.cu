@@ -368,6 +368,9 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
     return x <= z ? __ldg(P.a + static_cast<long long>(x) * lda + z)
                   : __ldg(P.a + static_cast<long long>(z) * lda + x);
   };
+  auto aptr = [&](int x, int z) -> const double* {
+    return x <= z ? P.a + static_cast<long long>(x) * lda + z : P.a + static_cast<long long>(z) * lda + x;
+  };
   const bool timing = P.stats != nullptr && t == 0;
   unsigned long long tm[6] = {0, 0, 0, 0, 0, 0};
   unsigned long long tmark = timing ? globaltimer_ns() : 0;
@@ -421,6 +424,9 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
   // reference's order (the last term, which involves the candidate's result
   // at column r, is added after the exchange), so results do not change.
   bool ahead = false;
+  // loaded one step ahead: the next row's coefficient column (ca) and the
+  // candidate's U column (cr), at most 2 * kThreads rows each
+  double ca0 = 0.0, ca1 = 0.0, cr0 = 0.0, cr1 = 0.0;
   double nx_omega = 0.0, nx_dpp = 0.0, nx_w1 = 0.0, nx_w2 = 0.0;
   int nx_r = 0, nx_rs = 0;
   double u_prev_r = 0.0, carry = 0.0;
@@ -512,17 +518,28 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
     // The next row's coefficient column (the visible rows q < nrel) is loaded
     // now for every slot the next row may have, so its latency hides behind
     // the rest of the step: A = slot of p+1, B = slot of p+2 (2x2 pivot),
-    // C = slot of p (r = p+1).
+    // C = slot of p (r = p+1).  After a row computed ahead, A (and the
+    // candidate's operands) were loaded by the previous step.
     const bool prefetch = lp <= 2 * kThreads;
-    auto preload = [&](int slot, double& c0, double& c1) {
+    auto preload = [&](int slot, int rows, double& c0, double& c1) {
       const double* ucol = P.uslot + static_cast<size_t>(slot) * ldu;
-      c0 = tz < nrel ? ldcg(ucol + tz) : 0.0;
-      c1 = tz + kThreads < nrel ? ldcg(ucol + tz + kThreads) : 0.0;
+      c0 = tz < rows ? ldcg(ucol + tz) : 0.0;
+      c1 = tz + kThreads < rows ? ldcg(ucol + tz + kThreads) : 0.0;
+    };
+    // the candidate column's operands for pivot row pp with candidate slot
+    // rslot: A(z, r) of this CTA's active slots into wcs, U[q, r] (q < rows) into cr
+    auto issue_cand = [&](int pp, int rslot, int rows) {
+#pragma unroll
+      for (int k = 0; k < kCols; ++k) {
+        const int z = lo + tz + k * kThreads;
+        if (z < hi && mypos[z - lo] >= pp) cp_async_8(&wcs[z - lo], aptr(z, rslot));
+      }
+      if (prefetch) preload(rslot, rows, cr0, cr1);
     };
     const int slot_a = lp + 1 < nwin ? win[lp + 1] : -1;
     int slot_b = -1, slot_c = -1;
-    double ca0 = 0.0, ca1 = 0.0, cb0 = 0.0, cb1 = 0.0, cc0 = 0.0, cc1 = 0.0;
-    if (prefetch && slot_a >= 0) preload(slot_a, ca0, ca1);
+    double cb0 = 0.0, cb1 = 0.0, cc0 = 0.0, cc1 = 0.0;
+    if (!was_ahead && prefetch && slot_a >= 0) preload(slot_a, nrel, ca0, ca1);
 
     int kind = 1;  // 1: 1x1 at p; -1: 1x1 after p<->r; 2: 2x2 with p+1<->r
     bool cand = false, spec = false;
@@ -534,88 +551,50 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
     if (!(fabs(dpp) >= xmul(kAlpha, omega) || omega == 0.0)) {
       cand = true;
       ++ncand;
+      if (!was_ahead) issue_cand(p, rs, nrel);
       slot_b = lp + 2 < nwin ? win[lp + 2] : -1;
       slot_c = r == p + 1 ? sp : -1;
-      if (prefetch && slot_b >= 0) preload(slot_b, cb0, cb1);
-      if (prefetch && slot_c >= 0) preload(slot_c, cc0, cc1);
+      if (prefetch && slot_b >= 0) preload(slot_b, nrel, cb0, cb1);
+      if (prefetch && slot_c >= 0) preload(slot_c, nrel, cc0, cc1);
       spec = r != p + 1 && p + 1 < P.nominal_end && slot_a >= 0;
-      // ---- candidate column W(i, r) = A(i, r) - sum_q U[q, r] W[q, i]
-      // (CopyCandidateToWorkspace + UpdateCandidateInWorkspace, :184-352)
-      double cv[kCols];
-#pragma unroll
-      for (int k = 0; k < kCols; ++k) {
-        const int z = lo + tz + k * kThreads;
-        cv[k] = (z < hi && mypos[z - lo] >= p) ? asym(z, rs) : 0.0;
-      }
-      double cr0 = 0.0, cr1 = 0.0;
-      if (prefetch) preload(rs, cr0, cr1);
-      // the candidate's coefficients U[q, r]: the visible rows from r's slot,
-      // then U[lp - 1, r] passed along by the previous step
-      auto put_cand_coef = [&]() {
-        if (prefetch) {
-          if (tz < nrel) coef[tz] = cr0;
-          if (tz + kThreads < nrel) coef[tz + kThreads] = cr1;
-        } else {
-          const double* ucol = P.uslot + static_cast<size_t>(rs) * ldu;
-          for (int q = t; q < nrel; q += kBlock) coef[q] = ldcg(ucol + q);
+      // coefficients: coef = U[q, r] (the candidate column), coef2 = U[q, p+1]
+      // (row p+1, when computed ahead; U[lp, p+1] is applied last); the
+      // visible rows from the slots' columns, then row lp - 1 passed along
+      if (prefetch) {
+        if (tz < nrel) {
+          coef[tz] = cr0;
+          coef2[tz] = ca0;
         }
-        if (was_ahead && t == 0) coef[lp - 1] = u_prev_r;
-      };
-      if (spec) {
-        // row p+1's coefficients U[q, p+1] for q < lp (U[lp, p+1] is applied last)
-        if (prefetch) {
-          if (tz < nrel) coef2[tz] = ca0;
-          if (tz + kThreads < nrel) coef2[tz + kThreads] = ca1;
-        } else {
-          const double* ucol = P.uslot + static_cast<size_t>(slot_a) * ldu;
-          for (int q = t; q < nrel; q += kBlock) coef2[q] = ldcg(ucol + q);
+        if (tz + kThreads < nrel) {
+          coef[tz + kThreads] = cr1;
+          coef2[tz + kThreads] = ca1;
         }
-        if (was_ahead && t == 0) coef2[lp - 1] = carry;
       } else {
-        put_cand_coef();
+        const double* ucol = P.uslot + static_cast<size_t>(rs) * ldu;
+        for (int q = t; q < nrel; q += kBlock) coef[q] = ldcg(ucol + q);
+        if (spec) {
+          const double* ucol2 = P.uslot + static_cast<size_t>(slot_a) * ldu;
+          for (int q = t; q < nrel; q += kBlock) coef2[q] = ldcg(ucol2 + q);
+        }
+      }
+      if (was_ahead && t == 0) {
+        coef[lp - 1] = u_prev_r;
+        coef2[lp - 1] = carry;
       }
       if (t < kMaxPub) s_pub[t] = 0.0;
+      cp_async_wait_all();
       __syncthreads();
       // release U row lp - 1 (written by the previous step, after its last exchange)
       if (was_ahead && t == kThreads) fence_acq_rel_gpu();
-      if (spec) {
-        // ---- row p+1 as keeping pivot p leaves it: W[p+1, j] = A(p+1, j) -
-        // (sum_{q < lp} U[q, p+1] W[q, j] + U[lp, p+1] W[lp, j]); at j = r,
-        // W[lp, r] becomes the candidate's W(p, r), so the owner publishes
-        // A(p+1, r) and the partial sum instead
-        const bool staged1 = (slot_a - kstart) == lp + 1;
-        const double e0 = div_or_zero(w_p1, safe_denominator(dpp));
-        Cand best = no_cand();
-#pragma unroll
-        for (int k = 0; k < kCols; ++k) {
-          const int z = lo + tz + k * kThreads;
-          if (z < hi) {
-            const int j = mypos[z - lo];
-            if (j > p) {
-              const double a1 = staged1 ? wat(lp + 1, z) : asym(slot_a, z);
-              const double part = kOrdered ? ordered_dot(coef2, lp, [&](int q) { return wat(q, z); })
-                                           : split_dot(coef2, lp, [&](int q) { return wat(q, z); });
-              if (j != r) {
-                const double wp = wat(lp, z);
-                const double v1 = xsub(a1, xadd(part, xmul(e0, wp)));
-                sv[k] = v1;
-                if (j > p + 1)
-                  argmax_join(best, Cand{fabs(v1), j, z, wp});
-                else
-                  s_pub[4] = v1;  // W[p+1, p+1]
-                if (j == p + 2) s_pub[5] = v1;
-                if (j == p + 3) s_pub[6] = v1;
-              } else {
-                s_pub[7] = a1;
-                s_pub[8] = part;
-              }
-            }
-          }
-        }
-        nx_best = best;
-        put_cand_coef();
-        __syncthreads();
-      }
+      // ---- candidate column W(i, r) = A(i, r) - sum_q U[q, r] W[q, i]
+      // (CopyCandidateToWorkspace + UpdateCandidateInWorkspace, :184-352), and
+      // row p+1 as keeping pivot p leaves it: W[p+1, j] = A(p+1, j) -
+      // (sum_{q < lp} U[q, p+1] W[q, j] + U[lp, p+1] W[lp, j]).  At j = r,
+      // W[lp, r] becomes the candidate's W(p, r), so the owner publishes
+      // A(p+1, r) and the partial sum instead.
+      const bool staged1 = spec && (slot_a - kstart) == lp + 1;
+      const double e0 = spec ? div_or_zero(w_p1, safe_denominator(dpp)) : 0.0;
+      Cand best = no_cand();
       double sig = 0.0;
 #pragma unroll
       for (int k = 0; k < kCols; ++k) {
@@ -623,9 +602,18 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
         if (z < hi) {
           const int i = mypos[z - lo];
           if (i >= p) {
-            const double acc = kOrdered ? ordered_dot(coef, lp, [&](int q) { return wat(q, z); })
-                                        : split_dot(coef, lp, [&](int q) { return wat(q, z); });
-            const double v = xsub(cv[k], acc);
+            const bool two = spec && i > p;
+            double acc, part = 0.0;
+            auto wq = [&](int q) { return wat(q, z); };
+            if (two) {
+              if (kOrdered)
+                ordered_dot2(coef, coef2, lp, wq, acc, part);
+              else
+                split_dot2(coef, coef2, lp, wq, acc, part);
+            } else {
+              acc = kOrdered ? ordered_dot(coef, lp, wq) : split_dot(coef, lp, wq);
+            }
+            const double v = xsub(wcs[z - lo], acc);
             wcs[z - lo] = v;
             if (i != r) {
               const double av2 = fabs(v);
@@ -636,9 +624,27 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
             if (i == p) s_pub[1] = v;
             if (i == p + 1) s_pub[2] = v;
             if (i == p + 2) s_pub[3] = v;
+            if (two) {
+              const double a1 = staged1 ? wat(lp + 1, z) : asym(slot_a, z);
+              if (i != r) {
+                const double wp = wat(lp, z);
+                const double v1 = xsub(a1, xadd(part, xmul(e0, wp)));
+                sv[k] = v1;
+                if (i > p + 1)
+                  argmax_join(best, Cand{fabs(v1), i, z, wp});
+                else
+                  s_pub[4] = v1;  // W[p+1, p+1]
+                if (i == p + 2) s_pub[5] = v1;
+                if (i == p + 3) s_pub[6] = v1;
+              } else {
+                s_pub[7] = a1;
+                s_pub[8] = part;
+              }
+            }
           }
         }
       }
+      nx_best = best;
       lap(2);
       int owners[kMaxPub] = {};
       owners[0] = owner(rs);
@@ -688,7 +694,27 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
       const double d = dpp;
       const double den = safe_denominator(d);
       double wr = 0.0;  // W[p+1, r] of the row computed ahead
-      if (spec) wr = xsub(nx_ar, xadd(nx_part, xmul(div_or_zero(w_p1, den), wc_p)));
+      if (spec) {
+        wr = xsub(nx_ar, xadd(nx_part, xmul(div_or_zero(w_p1, den), wc_p)));
+        // the next step starts from row p+1 and its argmax
+        Cand best = nx_best;
+        argmax_join(best, Cand{fabs(wr), r, rs, wc_p});
+        nx_omega = best.v;
+        nx_r = best.i;
+        nx_rs = best.s;
+        nx_dpp = nx_d;
+        nx_w1 = r == p + 2 ? wr : nx_1;
+        nx_w2 = r == p + 3 ? wr : nx_2;
+        u_prev_r = div_or_zero(best.pay, den);
+        carry = div_or_zero(r == p + 2 ? wc_p : w_p2, den);
+        ahead = true;
+        // the next step's operands load while this step scales: its next
+        // row's coefficient column (slot of p+2) and, when it evaluates a
+        // candidate, that candidate's A and U columns (visible rows q < lp)
+        const int slot_a2 = lp + 2 < nwin ? win[lp + 2] : -1;
+        if (prefetch && slot_a2 >= 0) preload(slot_a2, lp, ca0, ca1);
+        if (!(fabs(nx_dpp) >= xmul(kAlpha, nx_omega) || nx_omega == 0.0)) issue_cand(p + 1, nx_rs, lp);
+      }
 #pragma unroll
       for (int k = 0; k < kCols; ++k) {
         const int z = lo + tz + k * kThreads;
@@ -710,20 +736,6 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
       if (c == 0 && t == 0) {
         P.dlog[2 * lp] = d;
         P.ptype[p] = 1;
-      }
-      if (spec) {
-        // the next step starts from row p+1 and its argmax
-        Cand best = nx_best;
-        argmax_join(best, Cand{fabs(wr), r, rs, wc_p});
-        nx_omega = best.v;
-        nx_r = best.i;
-        nx_rs = best.s;
-        nx_dpp = nx_d;
-        nx_w1 = r == p + 2 ? wr : nx_1;
-        nx_w2 = r == p + 3 ? wr : nx_2;
-        u_prev_r = div_or_zero(best.pay, den);
-        carry = div_or_zero(r == p + 2 ? wc_p : w_p2, den);
-        ahead = true;
       }
       if (was_ahead && !cand) {
         // next row's coefficients: U[q, p+1] for q < lp - 1, then U[lp - 1, p+1]
@@ -822,7 +834,7 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
         cpre[0] = cc0;
         cpre[1] = cc1;
       } else {
-        preload(next, cpre[0], cpre[1]);
+        preload(next, nrel, cpre[0], cpre[1]);
       }
       // U row nrel, released by this step's candidate exchange
       if (n_old > nrel) {
@@ -835,6 +847,7 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
     lap(4);
   }
 
+  cp_async_wait_all();
   if (P.stats && t == 0)
     for (int k = 0; k < 5; ++k) atomicAdd(P.stats + 16 + 2048 + c * 5 + k, tm[k]);
   const int e = p;
