@@ -349,14 +349,16 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
   const long long lda = P.lda, ldw = P.ldw;
   const int ldu = P.ldu;
   auto owner = [&](int z) -> int { return (z - kstart) / S; };
-  // shared memory: two coefficient columns, candidate column of this CTA's slots,
+  // shared memory: two coefficient columns, candidate column and row computed
+  // ahead of this CTA's slots,
   // (when it fits) the slots' panel rows wsm[m*S + (z - lo)], then the maps
   double* coef = dsm;
   double* coef2 = dsm + P.coef_cap;  // coefficients of a row computed ahead
   double* wcs = dsm + 2 * P.coef_cap;
-  double* wsm = wcs + P.smem_cols;
+  double* svs = wcs + P.smem_cols;   // the row computed ahead, by slot
+  double* wsm = svs + P.smem_cols;
   int* win = reinterpret_cast<int*>(
-      wcs + P.smem_cols + (kSmemW ? static_cast<size_t>(P.win_rows) * P.smem_cols : 0));
+      wsm + (kSmemW ? static_cast<size_t>(P.win_rows) * P.smem_cols : 0));
   int* mypos = win + P.win_pad;  // index held by slot lo + zz
   auto wat = [&](int m, int z) -> double& {
     if (kSmemW) return wsm[m * S + (z - lo)];
@@ -544,7 +546,6 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
     int kind = 1;  // 1: 1x1 at p; -1: 1x1 after p<->r; 2: 2x2 with p+1<->r
     bool cand = false, spec = false;
     double wc_r = 0.0, wc_p = 0.0, wc_p1 = 0.0, wc_p2 = 0.0;
-    double sv[kCols] = {};  // row p+1 computed ahead (columns other than r)
     double nx_ar = 0.0, nx_part = 0.0, nx_d = 0.0, nx_1 = 0.0, nx_2 = 0.0;
     Cand nx_best = no_cand();
     // FactorPanel's test, :90-92
@@ -596,50 +597,76 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
       const double e0 = spec ? div_or_zero(w_p1, safe_denominator(dpp)) : 0.0;
       Cand best = no_cand();
       double sig = 0.0;
+      // slot z holding index i >= p, with its candidate sum acc and (two) the
+      // partial sum of row p+1
+      auto finish = [&](int z, int i, double acc, double part, bool two) {
+        const double v = xsub(wcs[z - lo], acc);
+        wcs[z - lo] = v;
+        if (i != r) {
+          const double av2 = fabs(v);
+          sig = (sig < av2) ? av2 : sig;  // std::max, FindCandidateColumnMax :354-367
+        } else {
+          s_pub[0] = v;
+        }
+        if (i == p) s_pub[1] = v;
+        if (i == p + 1) s_pub[2] = v;
+        if (i == p + 2) s_pub[3] = v;
+        if (two) {
+          const double a1 = staged1 ? wat(lp + 1, z) : asym(slot_a, z);
+          if (i != r) {
+            const double wp = wat(lp, z);
+            const double v1 = xsub(a1, xadd(part, xmul(e0, wp)));
+            svs[z - lo] = v1;
+            if (i > p + 1)
+              argmax_join(best, Cand{fabs(v1), i, z, wp});
+            else
+              s_pub[4] = v1;  // W[p+1, p+1]
+            if (i == p + 2) s_pub[5] = v1;
+            if (i == p + 3) s_pub[6] = v1;
+          } else {
+            s_pub[7] = a1;
+            s_pub[8] = part;
+          }
+        }
+      };
+      if (!kOrdered && S <= kThreads / 2) {
+        // two lanes per slot (lanes l and l + 16 of a warp), each summing
+        // about half of the rows
+        if (t < kThreads) {
+          const int zz = (t >> 5) * 16 + (t & 15);
+          const int half = (t >> 4) & 1;
+          const int i = zz < width ? mypos[zz] : -1;
+          const bool act = i >= p;
+          double acc = 0.0, part = 0.0;
+          if (act) {
+            const int h = (lp >> 3) << 2;
+            const int z = lo + zz;
+            split_dot2_range(coef, coef2, half ? h : 0, half ? lp : h, [&](int q) { return wat(q, z); },
+                             acc, part);
+          }
+          acc += __shfl_xor_sync(0xffffffffu, acc, 16);
+          part += __shfl_xor_sync(0xffffffffu, part, 16);
+          if (act && half == 0) finish(lo + zz, i, acc, part, spec && i > p);
+        }
+      } else {
 #pragma unroll
-      for (int k = 0; k < kCols; ++k) {
-        const int z = lo + tz + k * kThreads;
-        if (z < hi) {
-          const int i = mypos[z - lo];
-          if (i >= p) {
-            const bool two = spec && i > p;
-            double acc, part = 0.0;
-            auto wq = [&](int q) { return wat(q, z); };
-            if (two) {
-              if (kOrdered)
-                ordered_dot2(coef, coef2, lp, wq, acc, part);
-              else
-                split_dot2(coef, coef2, lp, wq, acc, part);
-            } else {
-              acc = kOrdered ? ordered_dot(coef, lp, wq) : split_dot(coef, lp, wq);
-            }
-            const double v = xsub(wcs[z - lo], acc);
-            wcs[z - lo] = v;
-            if (i != r) {
-              const double av2 = fabs(v);
-              sig = (sig < av2) ? av2 : sig;  // std::max, FindCandidateColumnMax :354-367
-            } else {
-              s_pub[0] = v;
-            }
-            if (i == p) s_pub[1] = v;
-            if (i == p + 1) s_pub[2] = v;
-            if (i == p + 2) s_pub[3] = v;
-            if (two) {
-              const double a1 = staged1 ? wat(lp + 1, z) : asym(slot_a, z);
-              if (i != r) {
-                const double wp = wat(lp, z);
-                const double v1 = xsub(a1, xadd(part, xmul(e0, wp)));
-                sv[k] = v1;
-                if (i > p + 1)
-                  argmax_join(best, Cand{fabs(v1), i, z, wp});
+        for (int k = 0; k < kCols; ++k) {
+          const int z = lo + tz + k * kThreads;
+          if (z < hi) {
+            const int i = mypos[z - lo];
+            if (i >= p) {
+              const bool two = spec && i > p;
+              double acc, part = 0.0;
+              auto wq = [&](int q) { return wat(q, z); };
+              if (two) {
+                if (kOrdered)
+                  ordered_dot2(coef, coef2, lp, wq, acc, part);
                 else
-                  s_pub[4] = v1;  // W[p+1, p+1]
-                if (i == p + 2) s_pub[5] = v1;
-                if (i == p + 3) s_pub[6] = v1;
+                  split_dot2(coef, coef2, lp, wq, acc, part);
               } else {
-                s_pub[7] = a1;
-                s_pub[8] = part;
+                acc = kOrdered ? ordered_dot(coef, lp, wq) : split_dot(coef, lp, wq);
               }
+              finish(z, i, acc, part, two);
             }
           }
         }
@@ -729,7 +756,7 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
               wv = wat(lp, z);
             }
             P.uslot[static_cast<size_t>(z) * ldu + lp] = div_or_zero(wv, den);
-            if (spec) wat(lp + 1, z) = j == r ? wr : sv[k];
+            if (spec) wat(lp + 1, z) = j == r ? wr : svs[z - lo];
           }
         }
       }
@@ -1131,12 +1158,13 @@ int launch_panel(const FactorPlan& plan, int panel, cudaStream_t s) {
   P.poll_ns = poll_ns;
   if (plan.grid > kMaxGrid)
     return set_error(BBK_ERR_INVALID_ARGUMENT, "panel grid %d exceeds %d", plan.grid, kMaxGrid);
-  // shared memory: two coefficient columns + candidate column + (if it fits) the
+  // shared memory: two coefficient columns + candidate column + row computed
+  // ahead + (if it fits) the
   // slots' panel rows, then the window map and the slot -> index map
   const int smax = (plan.n + plan.grid - 1) / plan.grid;
   P.coef_cap = static_cast<int>(align_up(static_cast<size_t>(plan.b) + 4, 2));
   P.smem_cols = smax;
-  const size_t base = (2 * static_cast<size_t>(P.coef_cap) + smax) * sizeof(double) +
+  const size_t base = (2 * static_cast<size_t>(P.coef_cap) + 2 * static_cast<size_t>(smax)) * sizeof(double) +
                       (static_cast<size_t>(P.win_pad) + smax) * sizeof(int);
   const size_t wbytes = static_cast<size_t>(P.win_rows) * smax * sizeof(double);
   const size_t limit = 220 * 1024;
