@@ -129,16 +129,23 @@ __device__ __forceinline__ void argmax_join(Cand& a, const Cand& b) {
   if (b.v > a.v || (b.v == a.v && b.i < a.i)) a = b;
 }
 
+// Warp-wide argmax_join, every lane gets the result.  The values are never
+// negative or NaN, so their bit patterns order like the values: the maximum
+// comes from two integer reductions (high word, then low word among the
+// lanes that hold the highest high word), the index from a third.
 template <bool kPay>
 __device__ __forceinline__ void warp_argmax(Cand& c) {
-  for (int off = 16; off > 0; off >>= 1) {
-    Cand o;
-    o.v = __shfl_xor_sync(0xffffffffu, c.v, off);
-    o.i = __shfl_xor_sync(0xffffffffu, c.i, off);
-    o.s = __shfl_xor_sync(0xffffffffu, c.s, off);
-    o.pay = kPay ? __shfl_xor_sync(0xffffffffu, c.pay, off) : 0.0;
-    argmax_join(c, o);
-  }
+  const unsigned long long key = static_cast<unsigned long long>(__double_as_longlong(c.v));
+  const unsigned hi = static_cast<unsigned>(key >> 32), lo = static_cast<unsigned>(key);
+  const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
+  const unsigned mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
+  const bool top = hi == mhi && lo == mlo;
+  const unsigned midx = __reduce_min_sync(0xffffffffu, top ? static_cast<unsigned>(c.i) : 0xffffffffu);
+  const int who = __ffs(__ballot_sync(0xffffffffu, top && static_cast<unsigned>(c.i) == midx)) - 1;
+  c.v = __longlong_as_double(static_cast<long long>((static_cast<unsigned long long>(mhi) << 32) | mlo));
+  c.i = static_cast<int>(midx);
+  c.s = __shfl_sync(0xffffffffu, c.s, who);
+  if (kPay) c.pay = __shfl_sync(0xffffffffu, c.pay, who);
 }
 
 // Shared memory of the exchanges.
@@ -547,6 +554,7 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
     bool cand = false, spec = false;
     double wc_r = 0.0, wc_p = 0.0, wc_p1 = 0.0, wc_p2 = 0.0;
     double nx_ar = 0.0, nx_part = 0.0, nx_d = 0.0, nx_1 = 0.0, nx_2 = 0.0;
+    double e0 = 0.0;  // U[p, p+1] when p stays a 1x1 pivot (row computed ahead)
     Cand nx_best = no_cand();
     // FactorPanel's test, :90-92
     if (!(fabs(dpp) >= xmul(kAlpha, omega) || omega == 0.0)) {
@@ -594,7 +602,7 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
       // W[lp, r] becomes the candidate's W(p, r), so the owner publishes
       // A(p+1, r) and the partial sum instead.
       const bool staged1 = spec && (slot_a - kstart) == lp + 1;
-      const double e0 = spec ? div_or_zero(w_p1, safe_denominator(dpp)) : 0.0;
+      if (spec) e0 = div_or_zero(w_p1, safe_denominator(dpp));
       Cand best = no_cand();
       double sig = 0.0;
       // slot z holding index i >= p, with its candidate sum acc and (two) the
@@ -722,7 +730,7 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
       const double den = safe_denominator(d);
       double wr = 0.0;  // W[p+1, r] of the row computed ahead
       if (spec) {
-        wr = xsub(nx_ar, xadd(nx_part, xmul(div_or_zero(w_p1, den), wc_p)));
+        wr = xsub(nx_ar, xadd(nx_part, xmul(e0, wc_p)));
         // the next step starts from row p+1 and its argmax
         Cand best = nx_best;
         argmax_join(best, Cand{fabs(wr), r, rs, wc_p});
