@@ -203,10 +203,11 @@ __device__ __forceinline__ XResult exchange(const PanelArgs& P, unsigned tag, bo
     if (kTwo) X.pb[warp] = cb;
   }
   __syncthreads();  // also orders this CTA's global writes before a release
+  const unsigned long long t_stat = P.stats ? globaltimer_ns() : 0;
   unsigned long long* par_base =
       P.slots + static_cast<size_t>(tag & 1u) * kSlotWords * P.slot_stride;
   const size_t st = P.slot_stride;
-  const unsigned long long t0 = globaltimer_ns();
+  unsigned long long t0 = 0;  // read when a wait turns out to be long
   if (warp == kCommWarp) {
     Cand a = X.pa[0], b = kTwo ? X.pb[0] : no_cand();
     for (int k = 1; k < kWarps; ++k) {
@@ -243,6 +244,7 @@ __device__ __forceinline__ XResult exchange(const PanelArgs& P, unsigned tag, bo
       if (__all_sync(0xffffffffu, ld_acquire_u64(&P.st->xcount) >= target)) break;
       if (P.poll_ns) __nanosleep(P.poll_ns);
       if ((iter & 31u) == 0) {
+        if (iter == 32) t0 = globaltimer_ns();
         const bool stop = __any_sync(0xffffffffu, ld_relaxed_s32(&P.st->abort) != 0);
         const bool late = __any_sync(0xffffffffu, globaltimer_ns() - t0 > P.timeout_ns);
         if (stop || late) {
@@ -291,13 +293,14 @@ __device__ __forceinline__ XResult exchange(const PanelArgs& P, unsigned tag, bo
     if (pub_pending && static_cast<unsigned>(pw0 >> 32) == tag && static_cast<unsigned>(pw1 >> 32) == tag)
       pub_pending = false;
     if (!__any_sync(0xffffffffu, rec_pending || pub_pending)) break;
+    if (iter == 32) t0 = globaltimer_ns();
     if ((iter & 31u) == 0 && __any_sync(0xffffffffu, globaltimer_ns() - t0 > P.timeout_ns)) {
       if (lane == 0) fail(P.st, BBK_ERR_TIMEOUT);
       ok = false;
       break;
     }
   }
-  if (P.stats && blockIdx.x == 0 && t == kThreads) atomicAdd(P.stats + 7, globaltimer_ns() - t0);
+  if (P.stats && blockIdx.x == 0 && t == kThreads) atomicAdd(P.stats + 7, globaltimer_ns() - t_stat);
   // ---- reduce the records: per warp, then every thread over the warps
   Cand ra = no_cand(), rb = no_cand();
   if (has_rec && ok) {
@@ -349,6 +352,9 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
   const int n = P.n;
   const int kstart = ldcg(&P.st->kstart[P.panel & 1]);
   const int S = (n - kstart + G - 1) / G;  // slots per CTA
+  // reassociated modes with at most kThreads / 2 slots per CTA: two lanes
+  // (l and l + 16 of a warp) share each slot's candidate and look-ahead sums
+  const bool paired = !kOrdered && S <= kThreads / 2;
   const int lo = kstart + c * S;
   const int hi = min(n, lo + S);
   const int width = max(0, hi - lo);
@@ -536,12 +542,20 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
       c1 = tz + kThreads < rows ? ldcg(ucol + tz + kThreads) : 0.0;
     };
     // the candidate column's operands for pivot row pp with candidate slot
-    // rslot: A(z, r) of this CTA's active slots into wcs, U[q, r] (q < rows) into cr
+    // rslot: A(z, r) of this CTA's active slots into wcs, each copied by the
+    // thread that later finishes that slot; U[q, r] (q < rows) into cr
     auto issue_cand = [&](int pp, int rslot, int rows) {
+      if (paired) {
+        if (t < kThreads && ((t >> 4) & 1) == 0) {
+          const int zz = (t >> 5) * 16 + (t & 15);
+          if (zz < width && mypos[zz] >= pp) cp_async_8(&wcs[zz], aptr(lo + zz, rslot));
+        }
+      } else {
 #pragma unroll
-      for (int k = 0; k < kCols; ++k) {
-        const int z = lo + tz + k * kThreads;
-        if (z < hi && mypos[z - lo] >= pp) cp_async_8(&wcs[z - lo], aptr(z, rslot));
+        for (int k = 0; k < kCols; ++k) {
+          const int z = lo + tz + k * kThreads;
+          if (z < hi && mypos[z - lo] >= pp) cp_async_8(&wcs[z - lo], aptr(z, rslot));
+        }
       }
       if (prefetch) preload(rslot, rows, cr0, cr1);
     };
@@ -591,7 +605,6 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
         coef2[lp - 1] = carry;
       }
       if (t < kMaxPub) s_pub[t] = 0.0;
-      cp_async_wait_all();
       __syncthreads();
       // release U row lp - 1 (written by the previous step, after its last exchange)
       if (was_ahead && t == kThreads) fence_acq_rel_gpu();
@@ -608,6 +621,7 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
       // slot z holding index i >= p, with its candidate sum acc and (two) the
       // partial sum of row p+1
       auto finish = [&](int z, int i, double acc, double part, bool two) {
+        cp_async_wait_all();  // this thread's copy of A(z, r)
         const double v = xsub(wcs[z - lo], acc);
         wcs[z - lo] = v;
         if (i != r) {
@@ -637,7 +651,7 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
           }
         }
       };
-      if (!kOrdered && S <= kThreads / 2) {
+      if (paired) {
         // two lanes per slot (lanes l and l + 16 of a warp), each summing
         // about half of the rows
         if (t < kThreads) {
