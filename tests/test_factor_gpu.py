@@ -76,6 +76,21 @@ def test_random_factorizations_bitwise_ordered(cuda, bbk, port):
             assert np.array_equal(got.perm, want.perm) and np.array_equal(got.pivot_types, want.pivot_types)
 
 
+def test_non_finite_entries_bitwise_ordered(cuda, bbk, port):
+    # NaN / inf entries: the argmax never picks a NaN (strict '>' in the
+    # reference's scans), so factors (NaN where NaN), pivots and permutation
+    # follow the reference exactly.
+    for k, (i, j, v) in enumerate(((3, 7, np.nan), (0, 5, np.inf), (4, 4, np.nan), (1, 9, -np.inf))):
+        a = port.random_symmetric(12, 777 + k)
+        a[i, j] = a[j, i] = v
+        for b in (1, 3, 5, 12):
+            want = port.factor(a, b)
+            got = bbk.factor_host(a, b, mode="fp64_ordered")
+            assert np.array_equal(np.triu(got.factors), np.triu(want.factors), equal_nan=True), (i, j, v, b)
+            assert np.array_equal(got.perm, want.perm), (i, j, v, b)
+            assert np.array_equal(got.pivot_types, want.pivot_types), (i, j, v, b)
+
+
 def test_scale_sweep(cuda, bbk, port):
     # tests/block_ldlt_decomposition_test.cc:40-99: value scales 1e-12 .. 1e12
     scales = [1e-12, 1e-9, 1e-6, 1e-3, 1.0, 1e3, 1e6, 1e9, 1e12]

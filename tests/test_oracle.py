@@ -81,6 +81,18 @@ def test_scale_sweep_vs_reference(port, reference):
                 assert relative_error(port.reconstruct(fp), a) < TOLERANCE
 
 
+def test_non_finite_entries_vs_reference(port, reference):
+    # NaN / inf entries: pins the oracle's argmax (a NaN never wins) and its
+    # NaN propagation to the reference itself
+    for k, (i, j, v) in enumerate(((3, 7, np.nan), (0, 5, np.inf), (4, 4, np.nan), (1, 9, -np.inf))):
+        a = port.random_symmetric(12, 777 + k)
+        a[i, j] = a[j, i] = v
+        for b in (1, 3, 5, 12):
+            fp, fr = port.factor(a, b), reference.factor(a, b)
+            assert np.array_equal(np.triu(fp.factors), np.triu(fr.factors), equal_nan=True), (i, j, v, b)
+            assert np.array_equal(fp.perm, fr.perm) and np.array_equal(fp.pivot_types, fr.pivot_types)
+
+
 def test_solve_restatement(port):
     a = uniform_symmetric(60, 3)
     f = port.factor(a, 8)
