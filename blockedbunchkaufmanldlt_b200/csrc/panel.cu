@@ -209,11 +209,11 @@ __device__ __forceinline__ XResult exchange(const PanelArgs& P, unsigned tag, bo
   const size_t st = P.slot_stride;
   unsigned long long t0 = 0;  // read when a wait turns out to be long
   if (warp == kCommWarp) {
-    Cand a = X.pa[0], b = kTwo ? X.pb[0] : no_cand();
-    for (int k = 1; k < kWarps; ++k) {
-      argmax_join(a, X.pa[k]);
-      if (kTwo) argmax_join(b, X.pb[k]);
-    }
+    // one compute warp's partial per lane, reduced across the warp
+    Cand a = lane < kWarps ? X.pa[lane] : no_cand();
+    Cand b = kTwo && lane < kWarps ? X.pb[lane] : no_cand();
+    warp_argmax<false>(a);
+    if (kTwo) warp_argmax<true>(b);
     if (lane == 0 && release) fence_acq_rel_gpu();
     if (lane < kRec + 2 * npub) {
       unsigned word;
@@ -320,15 +320,12 @@ __device__ __forceinline__ XResult exchange(const PanelArgs& P, unsigned tag, bo
   }
   if (has_pub) X.pub[lane] = join_hi_lo(pw0, pw1);
   __syncthreads();
-  r.a = X.ra[0];
-  r.b = kTwo ? X.rb[0] : no_cand();
-  r.ok = X.ok[0] != 0;
-#pragma unroll
-  for (int k = 1; k < kAllWarps; ++k) {
-    argmax_join(r.a, X.ra[k]);
-    if (kTwo) argmax_join(r.b, X.rb[k]);
-    r.ok = r.ok && X.ok[k] != 0;
-  }
+  // every warp reduces the per-warp partials (one per lane)
+  r.a = lane < kAllWarps ? X.ra[lane] : no_cand();
+  r.b = kTwo && lane < kAllWarps ? X.rb[lane] : no_cand();
+  warp_argmax<false>(r.a);
+  if (kTwo) warp_argmax<true>(r.b);
+  r.ok = __all_sync(0xffffffffu, lane >= kAllWarps || X.ok[lane] != 0);
   return r;
 }
 
