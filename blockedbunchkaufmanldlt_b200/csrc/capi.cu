@@ -504,19 +504,43 @@ int bbk_factor_solve_host(int n, int block_size, double* a, long long lda, int* 
   } else {
     rc = bbk_factor_device_async(n, block_size, d_a, lda, d_perm, d_pt, d_pe, update_mode, ws, fws,
                                  d_status, s);
+    // The solve only reads the factors, so their copy back to the host runs
+    // on a second stream, concurrently with the solve.
+    cudaStream_t s2 = nullptr;
+    cudaEvent_t factored = nullptr, copied = nullptr;
+    if (!rc) {
+      err = cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking);
+      if (err == cudaSuccess) err = cudaEventCreateWithFlags(&factored, cudaEventDisableTiming);
+      if (err == cudaSuccess) err = cudaEventCreateWithFlags(&copied, cudaEventDisableTiming);
+      if (err == cudaSuccess) err = cudaEventRecord(factored, s);
+      if (err != cudaSuccess) rc = cuda_error(err, "factorization copy stream");
+    }
     if (!rc && nrhs > 0) rc = enqueue_solve(n, d_a, lda, d_perm, d_pt, nrhs, d_b, ldb,
                                             reinterpret_cast<double*>(ws), s);
     if (!rc) {
-      err = copy_upper(a, d_a, n, lda, cudaMemcpyDeviceToHost, s);
-      if (err == cudaSuccess) err = cudaMemcpyAsync(perm, d_perm, n * sizeof(int), cudaMemcpyDeviceToHost, s);
-      if (err == cudaSuccess) err = cudaMemcpyAsync(pivot_types, d_pt, n * sizeof(int), cudaMemcpyDeviceToHost, s);
+      // the second stream's copies are enqueued first: a copy into pageable
+      // memory (the status word below, or a caller's pageable buffer) can
+      // block this thread until its stream reaches it
+      err = cudaStreamWaitEvent(s2, factored, 0);
+      if (err == cudaSuccess) err = copy_upper(a, d_a, n, lda, cudaMemcpyDeviceToHost, s2);
+      if (err == cudaSuccess) err = cudaMemcpyAsync(perm, d_perm, n * sizeof(int), cudaMemcpyDeviceToHost, s2);
+      if (err == cudaSuccess) err = cudaMemcpyAsync(pivot_types, d_pt, n * sizeof(int), cudaMemcpyDeviceToHost, s2);
       if (err == cudaSuccess && panel_end)
-        err = cudaMemcpyAsync(panel_end, d_pe, nb * sizeof(int), cudaMemcpyDeviceToHost, s);
+        err = cudaMemcpyAsync(panel_end, d_pe, nb * sizeof(int), cudaMemcpyDeviceToHost, s2);
       if (err == cudaSuccess && nrhs > 0) err = cudaMemcpyAsync(b, d_b, bbytes, cudaMemcpyDeviceToHost, s);
       if (err == cudaSuccess) err = cudaMemcpyAsync(&h_status, d_status, sizeof(int), cudaMemcpyDeviceToHost, s);
+      if (err == cudaSuccess) err = cudaStreamSynchronize(s2);
       if (err == cudaSuccess) err = cudaStreamSynchronize(s);
       if (err != cudaSuccess) rc = cuda_error(err, "factorization");
     }
+    if (s2) {
+      // the frees below are ordered on s: s waits for s2's copies first
+      if (copied && cudaEventRecord(copied, s2) == cudaSuccess) cudaStreamWaitEvent(s, copied, 0);
+      cudaStreamSynchronize(s2);
+      cudaStreamDestroy(s2);
+    }
+    if (factored) cudaEventDestroy(factored);
+    if (copied) cudaEventDestroy(copied);
   }
   cudaFreeAsync(d_a, s);
   if (d_b) cudaFreeAsync(d_b, s);
