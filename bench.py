@@ -378,6 +378,25 @@ def run_b200(args):
             traffic = None
     roofline = {"kernel": dom, "bound": dk["bound"], "achieved": dk["achieved"], "peak": dk["peak"],
                 "unit": dk["unit"], "frac": dk["frac"], "traffic": traffic, "peak_source": dk["peak_source"]}
+    if dom == "panel":
+        # The panel is a chain of pivot steps, each needing one grid-wide
+        # exchange (argmax + published scalars) before the next can start:
+        # its floor is one bare exchange per step, measured here on the same
+        # grid (bbk_probe_exchange_ns: back-to-back exchanges, each with a
+        # release fence).
+        import torch
+        sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+        grid = max(min(sms, -(-n // 64)), -(-n // 576))  # the panel launch's grid (64 columns per CTA)
+        try:
+            x_ns = bbk.probe_exchange_ns(int(grid), 2000)
+        except Exception:  # noqa: BLE001 - diagnostics only
+            x_ns = None
+        per_step_us = kernels["panel"]["ms"] * 1e3 / (args.steps * n)
+        if x_ns:
+            roofline["latency"] = {"unit": "us per pivot step", "achieved": per_step_us,
+                                   "floor": x_ns / 1e3, "frac": (x_ns / 1e3) / per_step_us,
+                                   "floor_source": "one bare grid exchange per pivot step, measured live",
+                                   "grid": int(grid)}
 
     # end to end through the host-buffer C ABI (pinned host memory)
     e2e = None
