@@ -21,7 +21,8 @@
 // Data during a panel:
 //   shared   the CTA's slice of the panel rows: row m starts as
 //            A[k0 + m, slot] (loaded once) and becomes W[k0 + m, slot] when
-//            pivot row m is updated; the candidate column; the maps.
+//            pivot row m is updated; the candidate column; the row computed
+//            ahead; two coefficient columns; the maps.
 //   Uslot    U[q, x] at Uslot[slot(x) * ldu + q].
 //   dlog     D of every pivot; ptype.
 // At the end the CTAs write W and U in final column order, publish the slot
@@ -30,9 +31,12 @@
 // finalize_kernel then writes the interchanged entries back, the
 // permutation, and the panel's compact factor rows.
 //
-// Per pivot step the grid meets once (no candidate) or twice (candidate
-// column needed), in an exchange (arrival counter + one record per CTA) that
-// is also the argmax reduction.
+// Per pivot step the grid meets in an exchange (arrival counter + one record
+// per CTA) that is also the argmax reduction: once for the row, and once more
+// when a candidate column is needed.  A candidate step also computes the next
+// row as keeping its pivot would leave it and reduces that row's argmax in
+// the same exchange, so when the pivot is kept (most steps of saddle-point
+// matrices) the next step starts without a row exchange.
 #include <climits>
 #include <cstdio>
 #include <cstdlib>
