@@ -56,6 +56,9 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU baseline sample time")
+    ap.add_argument("--matrix", default="spectral", choices=["spectral", "random"],
+                    help="mixed: the spectral matrix (n=20000, 16 RHS, condition ~1e8) or the random "
+                         "indefinite one (n=40000, block 256, 4 RHS)")
     ap.add_argument("--workload", default="kkt", choices=["kkt", "mixed", "batched"],
                     help="kkt: the headline FP64 factor+solve line; mixed: FP64 vs low-precision "
                          "updates + FP64 refinement on an ill-conditioned matrix (n=20000, 16 RHS); "
@@ -543,6 +546,21 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def random_indefinite_device(n: int, seed: int, device, nrhs: int):
+    """Entries uniform[-1, 1] (upper triangle mirrored) plus N(0, 0.01) on the
+    diagonal: a random symmetric indefinite matrix; nrhs right-hand sides
+    N(0, 1) as rows."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    a = torch.empty(n, n, dtype=torch.float64, device=device).uniform_(-1.0, 1.0, generator=g)
+    a = torch.triu(a)
+    a = a + torch.triu(a, 1).T
+    a.diagonal().add_(torch.randn(n, generator=g, dtype=torch.float64, device=device) * 0.1)
+    rhs = torch.randn(nrhs, n, generator=g, dtype=torch.float64, device=device)
+    return a, rhs
+
+
 def spectral_device(n: int, seed: int, device, lo=1e-4, hi=1e4):
     """A = Q diag(lam) Q^T, Q from the QR of a Gaussian matrix, |lam|
     log-uniform in [lo, hi], half the signs negative (condition ~ hi/lo)."""
@@ -570,9 +588,14 @@ def run_mixed(args):
     import blockedbunchkaufmanldlt_b200 as bbk
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(0)
-    n = args.n if args.n != 10000 else 20000
-    blk = args.block
-    a0, rhs = spectral_device(n, args.seed, dev)
+    rand = args.matrix == "random"
+    n = args.n if args.n != 10000 else (40000 if rand else 20000)
+    blk = args.block if (args.block != 128 or not rand) else 256
+    if rand:
+        a0, rhs = random_indefinite_device(n, args.seed, dev, 4)
+    else:
+        a0, rhs = spectral_device(n, args.seed, dev)
+    nrhs = rhs.shape[0]
     tol = 1e-12
 
     def berr(x):
@@ -602,7 +625,7 @@ def run_mixed(args):
         (x64, perm64, pt64), ms = timed(fp64_path)
     e64 = berr(x64)
     results["fp64"] = {"ms": ms, "backward_error": e64, "refine_steps": 0}
-    for mode in ("fp32", "bf16x3"):
+    for mode in (("fp32", "bf16x3", "bf16") if rand else ("fp32", "bf16x3")):
         for _ in range(1 + max(0, min(args.warmup, 1))):
             w = a0.clone()
 
@@ -619,10 +642,13 @@ def run_mixed(args):
                          "forward_error_vs_fp64": fe, "speedup_vs_fp64": results["fp64"]["ms"] / ms}
     line = {"metric": "time to backward error <= 1e-12, FP64 vs low-precision update + FP64 GMRES-IR",
             "unit": "ms", "higher_is_better": False, "n_gpus": 1, "dtype": "f64 (panel, residual) + update",
-            "data": "synthetic: A = Q diag(lam) Q^T, Q from QR of a seeded Gaussian, |lam| log-uniform "
-                    "[1e-4, 1e4], half negative; 16 RHS N(0,1)",
-            "config": {"workload": f"mixed precision, n={n}, block {blk}, 16 RHS, condition ~1e8",
-                       "n": n, "block_size": blk, "nrhs": 16},
+            "data": ("synthetic: seeded uniform[-1,1] symmetric plus N(0, 0.01) on the diagonal; "
+                     f"{nrhs} RHS N(0,1)") if rand else
+                    ("synthetic: A = Q diag(lam) Q^T, Q from QR of a seeded Gaussian, |lam| log-uniform "
+                     "[1e-4, 1e4], half negative; 16 RHS N(0,1)"),
+            "config": {"workload": (f"large FP64 vs mixed, random indefinite n={n}, block {blk}, {nrhs} RHS"
+                                    if rand else f"mixed precision, n={n}, block {blk}, 16 RHS, condition ~1e8"),
+                       "n": n, "block_size": blk, "nrhs": nrhs},
             "results": results}
     print(json.dumps(line), flush=True)
 
