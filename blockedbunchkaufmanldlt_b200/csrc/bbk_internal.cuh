@@ -319,5 +319,8 @@ struct FactorPlan {
   unsigned long long timeout_ns = 0;
   unsigned long long* stats = nullptr;  // optional per-phase panel timing
   double* scales = nullptr;  // BF16 update: 2 x (n/64 + 2) power-of-two scales
+  void* hsplit = nullptr;    // BF16 update: 2 operands x 3 terms x hstride BF16, split once per panel
+  int kpad = 0;              // BF16 update: panel width rounded up to 32 (k pitch of hsplit)
+  size_t hstride = 0;        // BF16 update: elements per operand term (n_pad x kpad)
 };
 }  // namespace bbk

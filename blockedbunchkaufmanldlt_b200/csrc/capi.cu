@@ -89,6 +89,9 @@ size_t carve_factor(FactorPlan& plan, char* base) {
   plan.gbuf2 = c.take<double>(static_cast<size_t>(npad) * plan.move_cap);
   plan.permbuf = c.take<int>(static_cast<size_t>(plan.move_cap));
   plan.scales = c.take<double>(2 * (static_cast<size_t>(n) / 64 + 2));
+  plan.kpad = static_cast<int>(align_up(static_cast<size_t>(b) + 1, 32));
+  plan.hstride = static_cast<size_t>(npad) * plan.kpad;
+  plan.hsplit = c.take<unsigned short>(2 * 3 * plan.hstride);
   c.take<int>(4);  // status word for the synchronous entry point
   return c.off;
 }

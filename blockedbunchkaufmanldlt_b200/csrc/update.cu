@@ -559,6 +559,252 @@ int launch_mma(const UpdArgs& U, int grid, cudaStream_t s) {
 
 __global__ void block_scale_kernel(UpdArgs U, double* a_scale, double* b_scale);
 
+// ---------------------------------------------------------------------------
+// BF16 update of the factorization, split once per panel.  split_kernel
+// writes the panel's operands, scaled by the 64-block powers of two, as
+// kTerms BF16 terms in global memory, k contiguous and zero-padded to kpad:
+//   ah[t][(i - tile_i0) * kpad + k]  = term t of a_scale(i) * U(i, k)
+//   bh[t][(j - tile_i0) * kpad + k]  = term t of b_scale(j) * W(k, j)
+// (rows outside [i_lo, n) and k >= inner are zero), so the tile kernel only
+// loads BF16 and issues MMAs: converting in its inner loop put an FP64
+// multiply and an FP64 -> FP32 conversion per operand per warp on the FP64
+// pipe, which then limited the tensor cores.
+// ---------------------------------------------------------------------------
+constexpr int kSplitTile = 32;
+
+template <int kTerms>
+__global__ void __launch_bounds__(256) split_kernel(UpdArgs U, __nv_bfloat16* ah, __nv_bfloat16* bh, int kpad,
+                                                    size_t term_stride) {
+  __shared__ double tile[kSplitTile][kSplitTile + 1];
+  if (!resolve_range(U)) return;
+  const int rows = U.n - U.tile_i0;
+  const int rt = (rows + kSplitTile - 1) / kSplitTile, kt = kpad / kSplitTile;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+  for (int blk = blockIdx.x; blk < 2 * rt * kt; blk += gridDim.x) {
+    const bool is_a = blk < rt * kt;
+    const int b2 = is_a ? blk : blk - rt * kt;
+    const int r0 = (b2 / kt) * kSplitTile, k0 = (b2 % kt) * kSplitTile;
+    // load the 32 x 32 block (rows r0.., k k0..) scaled; A reads along k, B along the rows
+    for (int yy = ty; yy < kSplitTile; yy += 8) {
+      int r, k;
+      if (is_a) {
+        r = r0 + yy;
+        k = k0 + tx;
+      } else {
+        r = r0 + tx;
+        k = k0 + yy;
+      }
+      const int c = U.tile_i0 + r;
+      double v = 0.0;
+      if (r < rows && c >= U.i_lo && k < U.inner) {
+        const double sc = (is_a ? U.a_scale : U.b_scale)[r / kBM];
+        v = sc * (is_a ? U.a[static_cast<long long>(c) * U.a_si + k] : U.b[static_cast<long long>(k) * U.b_sk + c]);
+      }
+      if (is_a)
+        tile[yy][tx] = v;  // [row][k]
+      else
+        tile[tx][yy] = v;  // [row][k]
+    }
+    __syncthreads();
+    __nv_bfloat16* dst = is_a ? ah : bh;
+    for (int yy = ty; yy < kSplitTile; yy += 8) {
+      const int r = r0 + yy, k = k0 + tx;
+      if (r < rows) {
+        float rest = static_cast<float>(tile[yy][tx]);
+#pragma unroll
+        for (int t = 0; t < kTerms; ++t) {
+          const __nv_bfloat16 h = __float2bfloat16_rn(rest);
+          dst[t * term_stride + static_cast<size_t>(r) * kpad + k] = h;
+          rest -= __bfloat162float(h);
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+constexpr int kHPitch = kBK + 8;  // BF16 per smem row: 20 words, conflict-free fragment loads
+
+template <int kTerms>
+struct HSmem {
+  static constexpr int kOp = kTerms * kBM * kHPitch;  // one operand of one stage
+  static constexpr int kStage = 2 * kOp;
+  static constexpr size_t kBytes = 2 * kStage * sizeof(__nv_bfloat16);
+};
+
+__device__ __forceinline__ void cp_async_16h(__nv_bfloat16* smem_dst, const __nv_bfloat16* gsrc, bool valid) {
+  const unsigned saddr = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(saddr), "l"(gsrc), "r"(valid ? 16 : 0)
+               : "memory");
+}
+
+template <int kTerms>
+__device__ __forceinline__ void load_stage_h(const UpdArgs& U, const __nv_bfloat16* ah, const __nv_bfloat16* bh,
+                                             int kpad, size_t term_stride, __nv_bfloat16* st, int i0, int j0,
+                                             int k0) {
+  using Hs = HSmem<kTerms>;
+  const int rows = U.n - U.tile_i0;
+  constexpr int kChunks = kBM * (kBK / 8);  // 16-byte chunks per operand per term
+  for (int c = threadIdx.x; c < 2 * kTerms * kChunks; c += kThreadsMma) {
+    const int op = c / (kTerms * kChunks);
+    const int rem = c - op * (kTerms * kChunks);
+    const int t = rem / kChunks, q = rem - t * kChunks;
+    const int rr = q / (kBK / 8), kk = (q % (kBK / 8)) * 8;
+    const int r = (op == 0 ? i0 : j0) - U.tile_i0 + rr;
+    const bool ok = r < rows;
+    const __nv_bfloat16* src = (op == 0 ? ah : bh) + t * term_stride +
+                               static_cast<size_t>(ok ? r : 0) * kpad + k0 + kk;
+    cp_async_16h(st + op * Hs::kOp + (t * kBM + rr) * kHPitch + kk, src, ok);
+  }
+}
+
+template <int kTerms>
+__global__ void __launch_bounds__(kThreadsMma) bf16s_update_kernel(UpdArgs U, const __nv_bfloat16* ah,
+                                                                   const __nv_bfloat16* bh, int kpad,
+                                                                   size_t term_stride, int vec) {
+  using Hs = HSmem<kTerms>;
+  extern __shared__ __align__(16) __nv_bfloat16 hsm[];
+  if (!resolve_range(U)) return;
+  const int ntiles = tile_count(U);
+  int t = blockIdx.x;
+  if (t >= ntiles) return;
+  const int nchunks = (U.inner + kBK - 1) / kBK;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, tq = lane & 3;
+  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+  __nv_bfloat16* stage[2] = {hsm, hsm + Hs::kStage};
+  int I, J;
+  tile_coords(U, t, I, J);
+  int i0 = U.tile_i0 + I * kBM, j0 = U.tile_j0 + J * kBN;
+  load_stage_h<kTerms>(U, ah, bh, kpad, term_stride, stage[0], i0, j0, 0);
+  cp_async_commit();
+  int cur = 0;
+  for (;;) {
+    float acc[2][4][4];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.0f;
+    for (int ch = 0; ch < nchunks; ++ch) {
+      const int nxt = cur ^ 1;
+      if (ch + 1 < nchunks) {
+        load_stage_h<kTerms>(U, ah, bh, kpad, term_stride, stage[nxt], i0, j0, (ch + 1) * kBK);
+        cp_async_commit();
+        cp_async_wait<1>();
+      } else {
+        cp_async_wait<0>();
+      }
+      __syncthreads();  // chunk ch is in stage[cur]
+      const __nv_bfloat16* as = stage[cur];
+      const __nv_bfloat16* bs = stage[cur] + Hs::kOp;
+#pragma unroll
+      for (int ks = 0; ks < kBK; ks += 16) {
+        unsigned af[kTerms][2][4], bf[kTerms][4][2];
+#pragma unroll
+        for (int tt = 0; tt < kTerms; ++tt) {
+#pragma unroll
+          for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              const int rr = wm + mt * 16 + g + 8 * (u & 1), kk = ks + 2 * tq + 8 * (u >> 1);
+              af[tt][mt][u] = *reinterpret_cast<const unsigned*>(as + (tt * kBM + rr) * kHPitch + kk);
+            }
+#pragma unroll
+          for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+              const int cc = wn + nt * 8 + g, kk = ks + 2 * tq + 8 * u;
+              bf[tt][nt][u] = *reinterpret_cast<const unsigned*>(bs + (tt * kBM + cc) * kHPitch + kk);
+            }
+        }
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+          for (int nt = 0; nt < 4; ++nt) {
+            // smallest products first
+#pragma unroll
+            for (int ia = kTerms - 1; ia >= 0; --ia)
+#pragma unroll
+              for (int ib = kTerms - 1; ib >= 0; --ib)
+                if (ia + ib <= kTerms - 1) mma_bf16_16x8x16(acc[mt][nt], af[ia][mt], bf[ib][nt]);
+          }
+      }
+      __syncthreads();  // every warp is done with stage[cur]
+      if (ch + 1 < nchunks) cur = nxt;
+    }
+    // prefetch the next tile's first chunk while this tile's C is updated
+    const int tn = t + static_cast<int>(gridDim.x);
+    int ni0 = 0, nj0 = 0;
+    if (tn < ntiles) {
+      int nI, nJ;
+      tile_coords(U, tn, nI, nJ);
+      ni0 = U.tile_i0 + nI * kBM;
+      nj0 = U.tile_j0 + nJ * kBN;
+      load_stage_h<kTerms>(U, ah, bh, kpad, term_stride, stage[cur ^ 1], ni0, nj0, 0);
+      cp_async_commit();
+    }
+    const double unscale = 1.0 / (U.a_scale[(i0 - U.tile_i0) / kBM] * U.b_scale[(j0 - U.tile_j0) / kBN]);
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int i = i0 + wm + mt * 16 + g + h * 8;
+        if (i < U.i_lo || i >= U.i_hi) continue;
+        double* crow = U.c + static_cast<long long>(i) * U.ldc;
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+          const int j = j0 + wn + nt * 8 + tq * 2;
+          const double v0 = static_cast<double>(acc[mt][nt][h * 2]) * unscale;
+          const double v1 = static_cast<double>(acc[mt][nt][h * 2 + 1]) * unscale;
+          const bool ok0 = j >= U.j_lo && j < U.j_hi && (!U.upper_only || i <= j);
+          const bool ok1 = j + 1 >= U.j_lo && j + 1 < U.j_hi && (!U.upper_only || i <= j + 1);
+          if (vec && ok0 && ok1) {
+            double2 cv = *reinterpret_cast<const double2*>(crow + j);
+            cv.x -= v0;
+            cv.y -= v1;
+            *reinterpret_cast<double2*>(crow + j) = cv;
+          } else {
+            if (ok0) crow[j] -= v0;
+            if (ok1) crow[j + 1] -= v1;
+          }
+        }
+      }
+    }
+    if (tn >= ntiles) break;
+    cur ^= 1;
+    t = tn;
+    i0 = ni0;
+    j0 = nj0;
+  }
+  cp_async_wait<0>();
+}
+
+template <int kTerms>
+int launch_bf16_split(const UpdArgs& U, __nv_bfloat16* buf, int kpad, size_t term_stride, int grid_mma, bool vec,
+                      cudaStream_t s) {
+  const int sms = device_sm_count();
+  __nv_bfloat16* ah = buf;
+  __nv_bfloat16* bh = buf + static_cast<size_t>(kTerms) * term_stride;
+  split_kernel<kTerms><<<4 * sms, 256, 0, s>>>(U, ah, bh, kpad, term_stride);
+  BBK_CUDA_TRY(cudaGetLastError());
+  count_launch();
+  const size_t bytes = HSmem<kTerms>::kBytes;
+  static bool attr_set[64] = {};
+  int dev = 0;
+  BBK_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64 || !attr_set[dev]) {
+    BBK_CUDA_TRY(cudaFuncSetAttribute(bf16s_update_kernel<kTerms>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(bytes)));
+    if (dev >= 0 && dev < 64) attr_set[dev] = true;
+  }
+  bf16s_update_kernel<kTerms><<<grid_mma, kThreadsMma, bytes, s>>>(U, ah, bh, kpad, term_stride, vec ? 1 : 0);
+  BBK_CUDA_TRY(cudaGetLastError());
+  count_launch();
+  return BBK_OK;
+}
+
 int launch_by_mode(const UpdArgs& U, int mode, bool ak, bool vec, int grid_mma, int grid_simt,
                    cudaStream_t s) {
   switch (mode) {
@@ -686,6 +932,20 @@ int launch_update(const FactorPlan& plan, int panel, cudaStream_t s) {
   // vector path needs 16-byte aligned rows: ldu, ldw, lda even and a/c 16-byte aligned
   const bool vec = (plan.ldu % 2 == 0) && (plan.ldw % 2 == 0) && (plan.lda % 2 == 0) &&
                    (reinterpret_cast<uintptr_t>(plan.a) % 16 == 0);
+  // BF16 modes: operands split once per panel (16-byte copies need the split
+  // buffer 16-byte aligned; a caller's unaligned workspace keeps the
+  // in-loop split)
+  if ((plan.mode == BBK_UPDATE_BF16 || plan.mode == BBK_UPDATE_BF16X3) && plan.hsplit != nullptr &&
+      reinterpret_cast<uintptr_t>(plan.hsplit) % 16 == 0 && vec) {
+    if (U.a_scale == nullptr) return set_error(BBK_ERR_LOGIC, "BF16 update without its scales");
+    block_scale_kernel<<<2 * sms, 256, 0, s>>>(U, const_cast<double*>(U.a_scale), const_cast<double*>(U.b_scale));
+    BBK_CUDA_TRY(cudaGetLastError());
+    count_launch();
+    auto* buf = static_cast<__nv_bfloat16*>(plan.hsplit);
+    return plan.mode == BBK_UPDATE_BF16
+               ? launch_bf16_split<1>(U, buf, plan.kpad, plan.hstride, grid_mma, vec, s)
+               : launch_bf16_split<3>(U, buf, plan.kpad, plan.hstride, grid_mma, vec, s);
+  }
   return launch_by_mode(U, plan.mode, true, vec, grid_mma, grid_simt, s);
 }
 
