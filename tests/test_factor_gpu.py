@@ -1,6 +1,6 @@
 """GPU parity of the factorization against the oracle.
 
-Bar (north star): the plain FP64 path reproduces the reference's pivot
+Bar: the plain FP64 path reproduces the reference's pivot
 sequence (pivot types and permutation) exactly unless a decision was a near
 tie, and its relative reconstruction residual is within 10x of the
 reference's and at most n * eps64 (on the reference's relative-error metric,

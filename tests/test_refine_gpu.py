@@ -1,7 +1,7 @@
 """GPU: mixed-precision trailing updates and FP64 iterative refinement (no
 reference counterpart: the reference is FP64 only and has no solve).  The
-target is the north star's: backward error <= 1e-12 from factors whose
-trailing updates ran in FP32 or BF16, with the residual always in FP64."""
+target: backward error <= 1e-12 from factors whose trailing updates ran in
+FP32 or BF16, with the residual always in FP64."""
 import numpy as np
 import pytest
 
