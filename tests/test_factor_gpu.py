@@ -10,7 +10,7 @@ reference-ordered update mode must be bitwise identical to the reference.
 import numpy as np
 import pytest
 
-from common import (FIXED, GOLDEN_4x4, GOLDEN_4x4_COMPACT, GOLDEN_4x4_PIVOTS, TOLERANCE,
+from common import (FIXED, GOLDEN_4x4, GOLDEN_4x4_COMPACT, GOLDEN_4x4_PIVOTS, TOLERANCE, kkt_matrix,
                     load_large_cases, load_small_cases, reconstruct, relative_error, uniform_symmetric,
                     upper_hash)
 
@@ -89,6 +89,37 @@ def test_non_finite_entries_bitwise_ordered(cuda, bbk, port):
             assert np.array_equal(np.triu(got.factors), np.triu(want.factors), equal_nan=True), (i, j, v, b)
             assert np.array_equal(got.perm, want.perm), (i, j, v, b)
             assert np.array_equal(got.pivot_types, want.pivot_types), (i, j, v, b)
+
+
+@pytest.mark.parametrize("n,h,b", [(800, 600, 32), (1200, 960, 64), (3000, 2400, 128)])
+def test_kkt_bitwise_ordered(cuda, bbk, port, n, h, b):
+    # Saddle-point matrices: most candidate steps keep their pivot, so most
+    # rows are computed ahead in the candidate phase; the ordered mode must
+    # still be the reference bit for bit, and the reassociated mode must
+    # take the same pivots.
+    a = kkt_matrix(n, h, 5 + n)
+    want = port.factor(a, b)
+    got = bbk.factor_host(a, b, mode="fp64_ordered")
+    assert np.array_equal(np.triu(got.factors), np.triu(want.factors))
+    assert np.array_equal(got.perm, want.perm) and np.array_equal(got.pivot_types, want.pivot_types)
+    assert np.array_equal(got.panel_end, want.panel_end)
+    fast = bbk.factor_host(a, b, mode="fp64")
+    assert np.array_equal(fast.pivot_types, want.pivot_types) and np.array_equal(fast.perm, want.perm)
+    res = relative_error(reconstruct(fast.factors, fast.perm, fast.pivot_types), a)
+    assert res < TOLERANCE, res
+
+
+@pytest.mark.parametrize("n,b,seed", [(900, 24, 77), (1100, 40, 78)])
+def test_boundary_shifts_bitwise_ordered(cuda, bbk, port, n, b, seed):
+    # uniform matrices with many 2x2 pivots: boundary shifts after rows
+    # computed ahead, candidates at p+2 / p+3, no-candidate steps after them
+    a = uniform_symmetric(n, seed)
+    want = port.factor(a, b)
+    got = bbk.factor_host(a, b, mode="fp64_ordered")
+    assert np.array_equal(np.triu(got.factors), np.triu(want.factors))
+    assert np.array_equal(got.perm, want.perm) and np.array_equal(got.pivot_types, want.pivot_types)
+    assert np.array_equal(got.panel_end, want.panel_end)
+    assert any(e != min(n, (k + 1) * b) for k, e in enumerate(want.panel_end))  # shifts happen
 
 
 def test_scale_sweep(cuda, bbk, port):
