@@ -153,32 +153,6 @@ __device__ __forceinline__ void ordered_dot2(const double* c1, const double* c2,
   s2 = a2;
 }
 
-// Reassociated sums over q in [q0, q1), eight q per pass with four FMA
-// accumulators per sum.
-template <typename WGet>
-__device__ __forceinline__ void split_dot2_range(const double* c1, const double* c2, int q0, int q1,
-                                                 WGet&& w, double& s1, double& s2) {
-  double a[4] = {0.0, 0.0, 0.0, 0.0}, b[4] = {0.0, 0.0, 0.0, 0.0};
-  int q = q0;
-  for (; q + 8 <= q1; q += 8) {
-    double x[8];
-#pragma unroll
-    for (int u = 0; u < 8; ++u) x[u] = w(q + u);
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      a[u & 3] = __fma_rn(c1[q + u], x[u], a[u & 3]);
-      b[u & 3] = __fma_rn(c2[q + u], x[u], b[u & 3]);
-    }
-  }
-  for (; q < q1; ++q) {
-    const double x = w(q);
-    a[0] = __fma_rn(c1[q], x, a[0]);
-    b[0] = __fma_rn(c2[q], x, b[0]);
-  }
-  s1 = (a[0] + a[1]) + (a[2] + a[3]);
-  s2 = (b[0] + b[1]) + (b[2] + b[3]);
-}
-
 // The reassociated counterpart of ordered_dot2: four FMA accumulators per sum.
 template <typename WGet>
 __device__ __forceinline__ void split_dot2(const double* c1, const double* c2, int count, WGet&& w,

@@ -55,6 +55,7 @@ constexpr int kWarps = kThreads / 32;  // compute warps
 constexpr int kCommWarp = kWarps;       // the communication warp
 constexpr int kBlock = kThreads + 32;   // compute warps + the communication warp
 constexpr int kCols = 3;  // slots per thread: S <= kCols * kThreads
+constexpr int kPairSlots = 96;  // slots per CTA up to which the warps split the candidate sums by rows
 constexpr int kAllWarps = kBlock / 32;
 constexpr int kMaxGrid = kBlock;  // CTAs of a panel launch: every thread reads one record
 constexpr int kRecA = 4;  // argmax words of a record: idx, value hi, value lo, slot
@@ -353,9 +354,9 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
   const int n = P.n;
   const int kstart = ldcg(&P.st->kstart[P.panel & 1]);
   const int S = (n - kstart + G - 1) / G;  // slots per CTA
-  // reassociated modes with at most kThreads / 2 slots per CTA: two lanes
-  // (l and l + 16 of a warp) share each slot's candidate and look-ahead sums
-  const bool paired = !kOrdered && S <= kThreads / 2;
+  // reassociated modes with at most kPairSlots slots per CTA: the compute
+  // warps split the rows of the candidate and look-ahead sums
+  const bool paired = !kOrdered && S <= kPairSlots;
   const int lo = kstart + c * S;
   const int hi = min(n, lo + S);
   const int width = max(0, hi - lo);
@@ -370,7 +371,8 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
   double* coef2 = dsm + P.coef_cap;  // coefficients of a row computed ahead
   double* wcs = dsm + 2 * P.coef_cap;
   double* svs = wcs + P.smem_cols;   // the row computed ahead, by slot
-  double* wsm = svs + P.smem_cols;
+  double* wpart = svs + P.smem_cols;  // per-warp partial sums: 2 x kWarps x kPairSlots
+  double* wsm = wpart + 2 * kWarps * kPairSlots;
   int* win = reinterpret_cast<int*>(
       wsm + (kSmemW ? static_cast<size_t>(P.win_rows) * P.smem_cols : 0));
   int* mypos = win + P.win_pad;  // index held by slot lo + zz
@@ -546,17 +548,10 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
     // rslot: A(z, r) of this CTA's active slots into wcs, each copied by the
     // thread that later finishes that slot; U[q, r] (q < rows) into cr
     auto issue_cand = [&](int pp, int rslot, int rows) {
-      if (paired) {
-        if (t < kThreads && ((t >> 4) & 1) == 0) {
-          const int zz = (t >> 5) * 16 + (t & 15);
-          if (zz < width && mypos[zz] >= pp) cp_async_8(&wcs[zz], aptr(lo + zz, rslot));
-        }
-      } else {
 #pragma unroll
-        for (int k = 0; k < kCols; ++k) {
-          const int z = lo + tz + k * kThreads;
-          if (z < hi && mypos[z - lo] >= pp) cp_async_8(&wcs[z - lo], aptr(z, rslot));
-        }
+      for (int k = 0; k < kCols; ++k) {
+        const int z = lo + tz + k * kThreads;
+        if (z < hi && mypos[z - lo] >= pp) cp_async_8(&wcs[z - lo], aptr(z, rslot));
       }
       if (prefetch) preload(rslot, rows, cr0, cr1);
     };
@@ -653,23 +648,46 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
         }
       };
       if (paired) {
-        // two lanes per slot (lanes l and l + 16 of a warp), each summing
-        // about half of the rows
+        // each compute warp sums a range of rows for every slot (lanes l,
+        // l + 32, l + 64), so each coefficient is read by one warp only; the
+        // per-warp partial sums are then added in warp order
         if (t < kThreads) {
-          const int zz = (t >> 5) * 16 + (t & 15);
-          const int half = (t >> 4) & 1;
-          const int i = zz < width ? mypos[zz] : -1;
-          const bool act = i >= p;
-          double acc = 0.0, part = 0.0;
-          if (act) {
-            const int h = (lp >> 3) << 2;
-            const int z = lo + zz;
-            split_dot2_range(coef, coef2, half ? h : 0, half ? lp : h, [&](int q) { return wat(q, z); },
-                             acc, part);
+          const int w = t >> 5, ln = t & 31;
+          const int qa = (lp * w) / kWarps, qb = (lp * (w + 1)) / kWarps;
+          double sa[3] = {0.0, 0.0, 0.0}, sb[3] = {0.0, 0.0, 0.0};
+          for (int q = qa; q < qb; ++q) {
+            const double c1 = coef[q], c2 = coef2[q];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+              const int zz = ln + 32 * k;
+              if (zz < width) {
+                const double x = wat(q, lo + zz);
+                sa[k] = __fma_rn(c1, x, sa[k]);
+                sb[k] = __fma_rn(c2, x, sb[k]);
+              }
+            }
           }
-          acc += __shfl_xor_sync(0xffffffffu, acc, 16);
-          part += __shfl_xor_sync(0xffffffffu, part, 16);
-          if (act && half == 0) finish(lo + zz, i, acc, part, spec && i > p);
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            const int zz = ln + 32 * k;
+            if (zz < width) {
+              wpart[(2 * w) * kPairSlots + zz] = sa[k];
+              wpart[(2 * w + 1) * kPairSlots + zz] = sb[k];
+            }
+          }
+        }
+        __syncthreads();
+        if (t < width) {
+          const int i = mypos[t];
+          if (i >= p) {
+            double acc = wpart[t], part = wpart[kPairSlots + t];
+#pragma unroll
+            for (int w = 1; w < kWarps; ++w) {
+              acc += wpart[(2 * w) * kPairSlots + t];
+              part += wpart[(2 * w + 1) * kPairSlots + t];
+            }
+            finish(lo + t, i, acc, part, spec && i > p);
+          }
         }
       } else {
 #pragma unroll
@@ -1187,7 +1205,8 @@ int launch_panel(const FactorPlan& plan, int panel, cudaStream_t s) {
   const int smax = (plan.n + plan.grid - 1) / plan.grid;
   P.coef_cap = static_cast<int>(align_up(static_cast<size_t>(plan.b) + 4, 2));
   P.smem_cols = smax;
-  const size_t base = (2 * static_cast<size_t>(P.coef_cap) + 2 * static_cast<size_t>(smax)) * sizeof(double) +
+  const size_t base = (2 * static_cast<size_t>(P.coef_cap) + 2 * static_cast<size_t>(smax) +
+                       2 * static_cast<size_t>(kWarps) * kPairSlots) * sizeof(double) +
                       (static_cast<size_t>(P.win_pad) + smax) * sizeof(int);
   const size_t wbytes = static_cast<size_t>(P.win_rows) * smax * sizeof(double);
   const size_t limit = 220 * 1024;
