@@ -166,6 +166,12 @@ struct XResult {
   bool ok;
 };
 
+// Barrier of the compute warps only (named barrier 1): the communication
+// warp may be inside a release fence meanwhile.
+__device__ __forceinline__ void compute_warps_sync() {
+  asm volatile("bar.sync 1, %0;" ::"n"(kThreads) : "memory");
+}
+
 __device__ __forceinline__ void cp_async_8(double* smem_dst, const double* gsrc) {
   const unsigned saddr = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(saddr), "l"(gsrc) : "memory");
@@ -491,22 +497,57 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
       // release the previous steps' U rows while the compute warps update the row
       if (t == kThreads) fence_acq_rel_gpu();
       Cand best = no_cand();
+      auto finish_row = [&](int z, int j, double a_val, double acc) {
+        const double wv = xsub(a_val, acc);
+        wat(lp, z) = wv;
+        if (j > p)
+          argmax_join(best, Cand{fabs(wv), j, z, 0.0});  // FindCurrentRowMax, :164-182
+        else
+          s_pub[0] = wv;  // W[p, p]
+        if (j == p + 1) s_pub[1] = wv;
+        if (j == p + 2) s_pub[2] = wv;
+      };
+      if (paired) {
+        // the compute warps split the rows q < lp (see the candidate phase)
+        if (t < kThreads) {
+          const int w = t >> 5, ln = t & 31;
+          const int qa = (lp * w) / kWarps, qb = (lp * (w + 1)) / kWarps;
+          double s1[3] = {0.0, 0.0, 0.0};
+          for (int q = qa; q < qb; ++q) {
+            const double c1 = coef[q];
 #pragma unroll
-      for (int k = 0; k < kCols; ++k) {
-        const int z = lo + tz + k * kThreads;
-        if (z < hi) {
-          const int j = mypos[z - lo];
+            for (int k = 0; k < 3; ++k) {
+              const int zz = ln + 32 * k;
+              if (zz < width) s1[k] = __fma_rn(c1, wat(q, lo + zz), s1[k]);
+            }
+          }
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            const int zz = ln + 32 * k;
+            if (zz < width) wpart[w * kPairSlots + zz] = s1[k];
+          }
+          compute_warps_sync();
+        }
+        if (t < width) {
+          const int j = mypos[t];
           if (j >= p) {
-            const double acc = kOrdered ? ordered_dot(coef, lp, [&](int q) { return wat(q, z); })
-                                        : split_dot(coef, lp, [&](int q) { return wat(q, z); });
-            const double wv = xsub(av[k], acc);
-            wat(lp, z) = wv;
-            if (j > p)
-              argmax_join(best, Cand{fabs(wv), j, z, 0.0});  // FindCurrentRowMax, :164-182
-            else
-              s_pub[0] = wv;  // W[p, p]
-            if (j == p + 1) s_pub[1] = wv;
-            if (j == p + 2) s_pub[2] = wv;
+            double acc = wpart[t];
+#pragma unroll
+            for (int w = 1; w < kWarps; ++w) acc += wpart[w * kPairSlots + t];
+            finish_row(lo + t, j, av[0], acc);
+          }
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < kCols; ++k) {
+          const int z = lo + tz + k * kThreads;
+          if (z < hi) {
+            const int j = mypos[z - lo];
+            if (j >= p) {
+              const double acc = kOrdered ? ordered_dot(coef, lp, [&](int q) { return wat(q, z); })
+                                          : split_dot(coef, lp, [&](int q) { return wat(q, z); });
+              finish_row(z, j, av[k], acc);
+            }
           }
         }
       }
@@ -675,8 +716,8 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
               wpart[(2 * w + 1) * kPairSlots + zz] = sb[k];
             }
           }
+          compute_warps_sync();
         }
-        __syncthreads();
         if (t < width) {
           const int i = mypos[t];
           if (i >= p) {
