@@ -32,6 +32,25 @@ def test_factor_solve_one_call_kkt(cuda, bbk):
     assert backward_error(a, x[:, None], rhs[:, None]) < 1e-14
 
 
+@pytest.mark.parametrize("kind", ["kkt", "uniform"])
+def test_factor_solve_one_call_returns_the_factors(cuda, bbk, kind):
+    # the one-call entry point copies the factors back on a second stream
+    # while it solves: they must be exactly the factorization's, with the
+    # strict lower triangle of the caller's matrix untouched
+    n, b = 1500, 64
+    a = kkt_matrix(n, 1200, seed=7) if kind == "kkt" else uniform_symmetric(n, 8)
+    a = a + np.tril(np.full((n, n), 3.25), -1)  # lower part the factorization must not touch
+    rhs = np.random.default_rng(2).standard_normal((n, 3))
+    fac, x = bbk.factor_solve_host(a, b, rhs)
+    ref = bbk.factor_host(a, b)
+    assert np.array_equal(np.triu(fac.factors), np.triu(ref.factors))
+    assert np.array_equal(np.tril(fac.factors, -1), np.tril(a, -1))
+    assert np.array_equal(fac.perm, ref.perm) and np.array_equal(fac.pivot_types, ref.pivot_types)
+    assert np.array_equal(fac.panel_end, ref.panel_end)
+    sym = np.triu(a) + np.triu(a, 1).T
+    assert backward_error(sym, x, rhs) < 1e-13
+
+
 def test_zero_pivot_gives_zero_component(cuda, bbk, port):
     a = np.diag([2.0, -3.0, 0.0, 5.0])
     rhs = np.array([2.0, 3.0, 1.0, 10.0])
