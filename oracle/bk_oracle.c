@@ -55,18 +55,27 @@ static void symmetric_move(double* a, long long lda, int n, int s, int r,
   for (int i = 0; i < rows_above; ++i) swap_d(&a[IDX(i, s, lda)], &a[IDX(i, r, lda)]);
 }
 
+/* Every dot product below is accumulated in its own variable, q ascending,
+ * starting from 0.0, exactly as the reference's scalar loops do; the loops
+ * are only nested with q outermost so the accumulators of a whole row
+ * advance together (contiguous, vectorisable loads).  The sequence of
+ * roundings each accumulator sees is unchanged, so results are too. */
 static int factor_impl(int n, int b, double* a, long long lda, int* perm,
                        int* pivot_types, int* panel_end, int* shifted,
-                       int max_panels) {
+                       int max_panels, double* log) {
   if (n <= 0 || b <= 0 || lda < n || !a || !perm || !pivot_types) return -1;
   const int nb = (n + b - 1) / b;
   double* w = (double*)calloc((size_t)(b + 1) * (size_t)n, sizeof(double));
   double* wc = (double*)calloc((size_t)n, sizeof(double));
-  if (!w || !wc) {
+  double* acc = (double*)calloc((size_t)n, sizeof(double));
+  if (!w || !wc || !acc) {
     free(w);
     free(wc);
+    free(acc);
     return -1;
   }
+  if (log)
+    for (size_t i = 0; i < (size_t)n * BKO_LOG_WORDS; ++i) log[i] = NAN;
   for (int i = 0; i < n; ++i) {
     perm[i] = i;
     pivot_types[i] = 0;
@@ -86,12 +95,13 @@ static int factor_impl(int n, int b, double* a, long long lda, int* perm,
       double* wp = w + (size_t)(p - k0) * n;
       /* CopyCurrentRowToWorkspace + UpdateCurrentRowInWorkspace (:122-162):
        * W[p,j] = A[p,j] - sum_{q<p in panel} U[q,p] W[q,j] */
-      for (int j = p; j < n; ++j) {
-        double update = 0.0;
-        for (int q = k0; q < p; ++q)
-          update += a[IDX(q, p, lda)] * w[IDX(q - k0, j, n)];
-        wp[j] = a[IDX(p, j, lda)] - update;
+      for (int j = p; j < n; ++j) acc[j] = 0.0;
+      for (int q = k0; q < p; ++q) {
+        const double c = a[IDX(q, p, lda)];
+        const double* wq = w + (size_t)(q - k0) * n;
+        for (int j = p; j < n; ++j) acc[j] += c * wq[j];
       }
+      for (int j = p; j < n; ++j) wp[j] = a[IDX(p, j, lda)] - acc[j];
       /* FindCurrentRowMax (:164-182): strict '>' in ascending column order,
        * so the lowest index wins ties and NaN never wins. */
       double omega = 0.0;
@@ -104,23 +114,44 @@ static int factor_impl(int n, int b, double* a, long long lda, int* perm,
         }
       }
       const double dpp = wp[p];
+      if (log) {
+        /* the decision quantities of this step (overwritten if the step is
+         * redone after a boundary shift); the runner-up of the row argmax
+         * shows how close another column came to being the candidate */
+        double second = 0.0;
+        for (int j = p + 1; j < n; ++j)
+          if (j != r && fabs(wp[j]) > second) second = fabs(wp[j]);
+        double* lg = log + (size_t)p * BKO_LOG_WORDS;
+        lg[0] = fabs(dpp);
+        lg[1] = omega;
+        lg[2] = second;
+        lg[3] = NAN;
+        lg[4] = NAN;
+      }
       int kind = 1; /* 1: 1x1 at p; -1: 1x1 after swapping p<->r; 2: 2x2 */
       int have_candidate = 0;
       if (!(fabs(dpp) >= BKO_ALPHA * omega || omega == 0.0)) {
         have_candidate = 1;
         /* CopyCandidateToWorkspace + UpdateCandidateInWorkspace (:184-352):
          * W(i,r) = A(i,r) - sum_q U[q,r] W[q,i] for every active i >= p. */
+        for (int i = p; i < n; ++i) acc[i] = 0.0;
+        for (int q = k0; q < p; ++q) {
+          const double c = a[IDX(q, r, lda)];
+          const double* wq = w + (size_t)(q - k0) * n;
+          for (int i = p; i < n; ++i) acc[i] += c * wq[i];
+        }
         for (int i = p; i < n; ++i) {
           const double aval = i <= r ? a[IDX(i, r, lda)] : a[IDX(r, i, lda)];
-          double update = 0.0;
-          for (int q = k0; q < p; ++q)
-            update += a[IDX(q, r, lda)] * w[IDX(q - k0, i, n)];
-          wc[i] = aval - update;
+          wc[i] = aval - acc[i];
         }
         /* FindCandidateColumnMax (:354-367) */
         double sigma = 0.0;
         for (int i = p; i < n; ++i)
           if (i != r) sigma = std_max(sigma, fabs(wc[i]));
+        if (log) {
+          log[(size_t)p * BKO_LOG_WORDS + 3] = sigma;
+          log[(size_t)p * BKO_LOG_WORDS + 4] = fabs(wc[r]);
+        }
         /* SelectPivot (:369-390) */
         if (fabs(dpp) * sigma - BKO_ALPHA * omega * omega >= 0.0) {
           kind = 1;
@@ -204,12 +235,14 @@ static int factor_impl(int n, int b, double* a, long long lda, int* perm,
      * upper triangle, q ascending, sum first then one subtraction. */
     if (e > k0) {
       for (int i = e; i < n; ++i) {
-        for (int j = i; j < n; ++j) {
-          double update = 0.0;
-          for (int q = k0; q < e; ++q)
-            update += a[IDX(q, i, lda)] * w[IDX(q - k0, j, n)];
-          a[IDX(i, j, lda)] -= update;
+        for (int j = i; j < n; ++j) acc[j] = 0.0;
+        for (int q = k0; q < e; ++q) {
+          const double c = a[IDX(q, i, lda)];
+          const double* wq = w + (size_t)(q - k0) * n;
+          for (int j = i; j < n; ++j) acc[j] += c * wq[j];
         }
+        double* ai = a + IDX(i, 0, lda);
+        for (int j = i; j < n; ++j) ai[j] -= acc[j];
       }
     }
     k0 = e;
@@ -217,13 +250,22 @@ static int factor_impl(int n, int b, double* a, long long lda, int* perm,
   }
   free(w);
   free(wc);
+  free(acc);
   return panels_done;
 }
 
 int bko_factor(int n, int block_size, double* a, long long lda, int* perm,
                int* pivot_types, int* panel_end, int* shifted) {
   const int r = factor_impl(n, block_size, a, lda, perm, pivot_types,
-                            panel_end, shifted, 1 << 30);
+                            panel_end, shifted, 1 << 30, NULL);
+  return r < 0 ? -1 : 0;
+}
+
+int bko_factor_logged(int n, int block_size, double* a, long long lda,
+                      int* perm, int* pivot_types, int* panel_end,
+                      int* shifted, double* log) {
+  const int r = factor_impl(n, block_size, a, lda, perm, pivot_types,
+                            panel_end, shifted, 1 << 30, log);
   return r < 0 ? -1 : 0;
 }
 
@@ -231,7 +273,7 @@ int bko_factor_panels(int n, int block_size, double* a, long long lda,
                       int* perm, int* pivot_types, int* panel_end,
                       int* shifted, int max_panels) {
   return factor_impl(n, block_size, a, lda, perm, pivot_types, panel_end,
-                     shifted, max_panels);
+                     shifted, max_panels, NULL);
 }
 
 void bko_scale_one_by_one(int count, double pivot, const double* source,

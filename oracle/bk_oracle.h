@@ -39,6 +39,24 @@ extern "C" {
 int bko_factor(int n, int block_size, double* a, long long lda, int* perm,
                int* pivot_types, int* panel_end, int* shifted);
 
+/* Same factorization, also recording the Bunch-Kaufman decision quantities
+ * of every pivot step in log[p * BKO_LOG_WORDS + .] for the factored position
+ * p where the step's pivot starts (NaN elsewhere, e.g. the second row of a
+ * 2x2 pivot):
+ *   [0] |W(p,p)|                         the diagonal tested against alpha*omega
+ *   [1] omega = max_{j>p} |W(p,j)|       (FindCurrentRowMax, :164-182)
+ *   [2] the runner-up of that argmax     (max over j>p, j != r)
+ *   [3] sigma = max_{i>=p,i!=r} |W(i,r)| (FindCandidateColumnMax, :354-367;
+ *                                         NaN when no candidate was needed)
+ *   [4] |W(r,r)|                         (NaN when no candidate was needed)
+ * From these, every comparison of FactorPanel (:90-92) and SelectPivot
+ * (:369-390) and its margin can be recomputed, so a decision that another
+ * summation order could flip (a near-tie) is visible. */
+#define BKO_LOG_WORDS 5
+int bko_factor_logged(int n, int block_size, double* a, long long lda,
+                      int* perm, int* pivot_types, int* panel_end,
+                      int* shifted, double* log);
+
 /* Same factorization, but stops after `max_panels` panels (used to time a
  * bounded sample of a large factorization).  Returns the number of panels
  * processed. */

@@ -66,6 +66,9 @@ class Port:
                                           ctypes.c_longlong, _ip, _ip, _ip, _ip,
                                           ctypes.c_int]
         lib.bko_factor_panels.restype = ctypes.c_int
+        lib.bko_factor_logged.argtypes = [ctypes.c_int, ctypes.c_int, _dp, ctypes.c_longlong,
+                                          _ip, _ip, _ip, _ip, _dp]
+        lib.bko_factor_logged.restype = ctypes.c_int
         lib.bko_solve.argtypes = [ctypes.c_int, _dp, ctypes.c_longlong, _ip, _ip,
                                   ctypes.c_int, _dp, ctypes.c_longlong]
         lib.bko_reconstruct.argtypes = [ctypes.c_int, _dp, ctypes.c_longlong, _ip, _ip, _dp]
@@ -106,6 +109,26 @@ class Port:
         if rc != 0:
             raise ValueError("oracle factorization rejected its arguments")
         return Factorization(f, perm, pt, pe, sh)
+
+    LOG_WORDS = 5  # BKO_LOG_WORDS
+
+    def factor_logged(self, a: np.ndarray, block_size: int):
+        """factor() plus the decision log of bko_factor_logged: an n x 5
+        array (|W(p,p)|, omega, runner-up of the row argmax, sigma, |W(r,r)|)
+        at every position where a pivot step started, NaN elsewhere."""
+        n = a.shape[0]
+        f = np.ascontiguousarray(a, dtype=np.float64).copy()
+        perm = np.zeros(n, np.int32)
+        pt = np.zeros(n, np.int32)
+        nb = (n + block_size - 1) // block_size
+        pe = np.zeros(nb, np.int32)
+        sh = np.zeros(nb, np.int32)
+        log = np.zeros((n, self.LOG_WORDS))
+        rc = self.lib.bko_factor_logged(n, block_size, _ptr(f), n, _ptr(perm, _ip), _ptr(pt, _ip),
+                                        _ptr(pe, _ip), _ptr(sh, _ip), _ptr(log))
+        if rc != 0:
+            raise ValueError("oracle factorization rejected its arguments")
+        return Factorization(f, perm, pt, pe, sh), log
 
     def solve(self, f: Factorization, b: np.ndarray) -> np.ndarray:
         n = f.factors.shape[0]

@@ -86,6 +86,75 @@ def kkt_matrix(n: int, h: int, seed: int, ridge: float = 1e-2) -> np.ndarray:
     return a
 
 
+def kkt_matrix_exact(n: int, h: int, seed: int, ridge: float = 1e-2):
+    """The saddle-point structure of kkt_matrix with an input that every
+    machine computes bit for bit: G's Gaussian entries are rounded to
+    multiples of 2^-10, so every product and partial sum of G G^T is an
+    integer multiple of 2^-20 below 2^39 in magnitude, exact in FP64 whatever
+    the BLAS's summation order, blocking or FMA use; the division by h and
+    the ridge are single IEEE roundings.  Returns (matrix, SHA-256 of its
+    bytes)."""
+    rng = np.random.default_rng(seed)
+    g = np.round(rng.standard_normal((h, h)) * 1024.0) / 1024.0
+    hm = g @ g.T
+    del g
+    hm /= h
+    hm[np.diag_indices(h)] += ridge
+    bm = rng.standard_normal((n - h, h))
+    a = np.zeros((n, n))
+    a[:h, :h] = hm
+    del hm
+    a[h:, :h] = bm
+    a[:h, h:] = bm.T
+    return a, hashlib.sha256(a.tobytes()).hexdigest()
+
+
+def relative_residual(a: np.ndarray, f: np.ndarray, perm: np.ndarray, pt: np.ndarray) -> float:
+    """||A - P^T L D L^T P||_F / ||A||_F from compact factors, vectorised
+    (L(i,k) = F(k,i) below the diagonal except inside a 2x2 pivot, D from
+    the diagonal and the (k,k+1) entries of 2x2 pivots)."""
+    n = f.shape[0]
+    two = np.where(np.asarray(pt) == 2)[0]
+    lt = np.triu(f, 1)
+    lt[two, two + 1] = 0.0
+    lt = lt.T.copy()
+    lt[np.diag_indices(n)] = 1.0
+    ld = lt * np.diag(f)[None, :]
+    ld[:, two] += lt[:, two + 1] * f[two, two + 1][None, :]
+    ld[:, two + 1] += lt[:, two] * f[two, two + 1][None, :]
+    m = ld @ lt.T
+    del ld, lt
+    rec = np.empty_like(m)
+    rec[np.ix_(perm, perm)] = m
+    del m
+    return float(np.linalg.norm(a - rec) / np.linalg.norm(a))
+
+
+ALPHA = 0.6403882032022076  # src/block_ldlt_decomposition.cc:14
+
+
+def reference_margins(log: np.ndarray) -> np.ndarray:
+    """Relative margins of the comparisons each pivot step of the reference
+    made, from the C restatement's decision log (oracle bko_factor_logged:
+    |W(p,p)|, omega, runner-up of the row argmax, sigma, |W(r,r)| per
+    position): the smallest |lhs - rhs| / max(|lhs|, |rhs|) over
+    |W(p,p)| >= alpha omega (:90-92), omega against its runner-up (the row
+    argmax, :164-182) and, after a candidate, the two SelectPivot tests
+    (:369-390).  NaN where no step started."""
+    d, om, second, sg, arr = (np.asarray(log[:, k], np.float64) for k in range(5))
+
+    def rel(x, y):
+        den = np.maximum(np.abs(x), np.abs(y))
+        with np.errstate(invalid="ignore", divide="ignore"):
+            return np.where(den > 0, np.abs(x - y) / np.where(den > 0, den, 1.0), np.inf)
+    with np.errstate(invalid="ignore"):
+        m = np.where(om == 0.0, np.inf, rel(d, ALPHA * om))
+        m = np.minimum(m, rel(om, second))
+        cand = ~np.isnan(sg)
+        m = np.where(cand, np.minimum(m, np.minimum(rel(d * sg, ALPHA * om * om), rel(arr, ALPHA * sg))), m)
+    return np.where(np.isnan(d), np.nan, m)
+
+
 def spectral_matrix(n: int, seed: int, lo: float = 1e-4, hi: float = 1e4) -> np.ndarray:
     """A = Q diag(lam) Q^T with Q from the QR of a Gaussian matrix, |lam|
     log-uniform in [lo, hi] and half of the signs negative (condition number

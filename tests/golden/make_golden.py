@@ -16,7 +16,18 @@ reference's outputs for an input that the tests can regenerate exactly:
   permutation, pivot types and compact upper factor (%.17g), read by
   tests/cpp/test_cpp_surface.cc.
 
-Usage: python tests/golden/make_golden.py
+* ``ref_kkt10000.npz`` (``--kkt``, a few minutes): the saddle-point
+  workload at full size (n=10000, H 8000, block 128) from
+  tests/common.py's kkt_matrix_exact, whose input every machine computes bit
+  for bit (its SHA-256 is stored and checked).  The reference's permutation,
+  pivot types, panel ends, a SHA-256 of its compact upper factor and its
+  relative reconstruction residual; the C restatement's per-step decision
+  log (oracle/bk_oracle.h, bko_factor_logged; float32) and the relative
+  margin of every decision computed from it in float64
+  (tests/common.py reference_margins), after checking that the restatement
+  reproduces the reference bit for bit on this input.
+
+Usage: python tests/golden/make_golden.py [--kkt]
 """
 import hashlib
 import json
@@ -64,7 +75,38 @@ def small_cases(port: Port):
     return cases
 
 
+KKT_CASE = {"n": 10000, "h": 8000, "block_size": 128, "seed": 20240}
+
+
+def kkt_parity_fixture():
+    sys.path.insert(0, os.path.dirname(HERE))
+    from common import kkt_matrix_exact, reference_margins, relative_residual
+    port, ref = Port(), Reference()
+    n, h, b, seed = (KKT_CASE[k] for k in ("n", "h", "block_size", "seed"))
+    a, a_sha = kkt_matrix_exact(n, h, seed)
+    r = ref.factor(a, b)
+    f, log = port.factor_logged(a, b)
+    assert upper_hash(f.factors) == upper_hash(r.factors), "restatement differs from the reference"
+    assert np.array_equal(f.perm, r.perm) and np.array_equal(f.pivot_types, r.pivot_types)
+    nbk = (n + b - 1) // b
+    ends = np.array([g[0] + g[1] for g in (r.geometry[bc + bc * (bc + 1) // 2] for bc in range(nbk))],
+                    np.int32)
+    assert np.array_equal(ends, f.panel_end)
+    res = relative_residual(a, r.factors, r.perm, r.pivot_types)
+    np.savez_compressed(os.path.join(HERE, "ref_kkt10000.npz"),
+                        n=n, h=h, block_size=b, seed=seed, input_sha256=a_sha,
+                        perm=r.perm, pivot_types=r.pivot_types.astype(np.int8), panel_end=ends,
+                        upper_sha256=upper_hash(r.factors), residual=res,
+                        reference_seconds=r.seconds, log=log.astype(np.float32),
+                        margin=reference_margins(log))
+    print(f"kkt n={n}: reference {r.seconds:.1f} s, residual {res:.3e}, "
+          f"{int((r.pivot_types == 1).sum())} 1x1 + {int((r.pivot_types == 2).sum())} 2x2 pivots")
+
+
 def main():
+    if "--kkt" in sys.argv:
+        kkt_parity_fixture()
+        return
     port, ref = Port(), Reference()
     out = {}
     names = []

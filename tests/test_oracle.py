@@ -100,3 +100,41 @@ def test_solve_restatement(port):
     b = rng.standard_normal((60, 3))
     x = port.solve(f, b)
     assert np.linalg.norm(a @ x - b) / np.linalg.norm(b) < 1e-10
+
+
+def test_decision_log_describes_each_step(port):
+    # bko_factor_logged: one record per pivot step at the position where its
+    # pivot starts; a step that needed no candidate passed the first test
+    # |W(p,p)| >= alpha omega (src/block_ldlt_decomposition.cc:90-92), one
+    # that did failed it; the second row of a 2x2 pivot has no record
+    from common import ALPHA
+    a = uniform_symmetric(300, 31)
+    f, log = port.factor_logged(a, 32)
+    plain = port.factor(a, 32)
+    assert np.array_equal(f.factors, plain.factors) and np.array_equal(f.perm, plain.perm)
+    pt = f.pivot_types
+    started = ~np.isnan(log[:, 0])
+    assert np.array_equal(started, pt != -2)
+    d, om, second, sg, arr = (log[started, k] for k in range(5))
+    cand = ~np.isnan(sg)
+    assert np.all((d >= ALPHA * om) | (om == 0.0) | cand)
+    assert np.all(d[cand] < ALPHA * om[cand])
+    assert np.all(second <= om)
+    assert np.array_equal(cand, ~np.isnan(arr))
+
+
+def test_oracle_reproduces_the_reference_kkt10000_fixture(port):
+    # The C restatement against the reference's own factorization of the
+    # full-size saddle-point workload (n=10000, block 128), stored by
+    # tests/golden/make_golden.py --kkt: identical factor bits, permutation,
+    # pivot types and panel ends (about a minute on one core).
+    import os
+    from common import GOLDEN, kkt_matrix_exact
+    z = np.load(os.path.join(GOLDEN, "ref_kkt10000.npz"))
+    a, sha = kkt_matrix_exact(int(z["n"]), int(z["h"]), int(z["seed"]))
+    assert sha == str(z["input_sha256"])
+    f = port.factor(a, int(z["block_size"]))
+    assert upper_hash(f.factors) == str(z["upper_sha256"])
+    assert np.array_equal(f.perm, z["perm"])
+    assert np.array_equal(f.pivot_types, z["pivot_types"].astype(np.int32))
+    assert np.array_equal(f.panel_end, z["panel_end"])
