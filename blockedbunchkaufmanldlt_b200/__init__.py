@@ -46,7 +46,7 @@ REFINE_GMRES = 1
 EXPORTS = (
     "bbk_abi_version", "bbk_last_error", "bbk_status_string", "bbk_kernel_launch_count",
     "bbk_set_wait_timeout_ns", "bbk_probe_bounded_wait", "bbk_probe_exchange_ns", "bbk_factor_workspace_size",
-    "bbk_factor_device", "bbk_factor_device_async", "bbk_factor_host",
+    "bbk_factor_device", "bbk_factor_device_async", "bbk_factor_device_logged", "bbk_factor_host",
     "bbk_solve_workspace_size", "bbk_solve_device", "bbk_solve_host", "bbk_factor_solve_host",
     "bbk_reconstruct_device", "bbk_scale_one_by_one", "bbk_scale_two_by_two",
     "bbk_update_trailing_block", "bbk_profile_begin", "bbk_profile_end", "bbk_panel_stats", "bbk_panel_stats_raw", "bbk_solve_device_noalloc",
@@ -134,6 +134,8 @@ def lib() -> ctypes.CDLL:
         "bbk_factor_device": ([_c_int, _c_int, _vp, _c_ll, _vp, _vp, _vp, _c_int, _vp, _c_sz, _vp], _c_int),
         "bbk_factor_device_async": ([_c_int, _c_int, _vp, _c_ll, _vp, _vp, _vp, _c_int, _vp, _c_sz,
                                      _vp, _vp], _c_int),
+        "bbk_factor_device_logged": ([_c_int, _c_int, _vp, _c_ll, _vp, _vp, _vp, _c_int, _vp, _vp, _c_sz,
+                                      _vp, _vp], _c_int),
         "bbk_factor_host": ([_c_int, _c_int, _vp, _c_ll, _vp, _vp, _vp, _c_int], _c_int),
         "bbk_solve_workspace_size": ([_c_int, _c_int], _c_sz),
         "bbk_solve_device": ([_c_int, _vp, _c_ll, _vp, _vp, _c_int, _vp, _c_ll, _vp, _c_sz, _vp], _c_int),
@@ -257,6 +259,60 @@ def factor_device(a, block_size: int, mode="fp64", stream=None, workspace=None,
                                             _stream_ptr(stream)))
         return perm, pt, pe, status
     return perm, pt, pe
+
+
+PIVOT_LOG_WORDS = 4  # |W(p,p)|, omega, sigma, |W(r,r)| per factored position
+ALPHA = 0.6403882032022076  # the Bunch-Kaufman threshold (1 + sqrt 17) / 8
+
+
+def factor_device_logged(a, block_size: int, mode="fp64", stream=None):
+    """factor_device plus the decision log of bbk_factor_device_logged:
+    returns (perm, pivot_types, panel_end, log) with log an n x 4 float64
+    device tensor (|W(p,p)|, omega, sigma, |W(r,r)| at each position where a
+    pivot step started; NaN elsewhere and where no candidate was needed)."""
+    import torch
+    if a.dtype != torch.float64 or not a.is_cuda or a.dim() != 2 or a.stride(1) != 1:
+        raise InvalidArgument(BBK_ERR_INVALID_ARGUMENT, "need a row-major CUDA float64 matrix")
+    n = a.shape[0]
+    nb = (n + block_size - 1) // block_size if block_size > 0 else 0
+    perm = torch.empty(n, dtype=torch.int32, device=a.device)
+    pt = torch.empty(n, dtype=torch.int32, device=a.device)
+    pe = torch.empty(max(nb, 1), dtype=torch.int32, device=a.device)
+    log = torch.empty(n, PIVOT_LOG_WORDS, dtype=torch.float64, device=a.device)
+    status = torch.zeros(1, dtype=torch.int32, device=a.device)
+    check(lib().bbk_factor_device_logged(n, block_size, ctypes.c_void_p(a.data_ptr()), a.stride(0),
+                                         ctypes.c_void_p(perm.data_ptr()), ctypes.c_void_p(pt.data_ptr()),
+                                         ctypes.c_void_p(pe.data_ptr()), _mode(mode),
+                                         ctypes.c_void_p(log.data_ptr()), None, 0,
+                                         ctypes.c_void_p(status.data_ptr()), _stream_ptr(stream)))
+    torch.cuda.current_stream().synchronize() if stream is None else stream.synchronize()
+    st = int(status.item())
+    if st != BBK_OK:
+        raise _EXC.get(st, BbkError)(st, "factorization aborted on the device")
+    return perm, pt, pe, log
+
+
+def decision_margins(log: np.ndarray) -> np.ndarray:
+    """Relative margin of the decision recorded at each position of a pivot
+    log (n x 4: |W(p,p)|, omega, sigma, |W(r,r)|): the smallest, over the
+    comparisons the step actually made, of |lhs - rhs| / max(|lhs|, |rhs|)
+    for |W(p,p)| >= alpha omega (src/block_ldlt_decomposition.cc:90-92) and,
+    after a candidate, |W(p,p)| sigma >= alpha omega^2 and |W(r,r)| >= alpha
+    sigma (SelectPivot, :369-390).  NaN where no step started.  A decision
+    whose margin is within rounding of zero could flip under another
+    summation order: a near-tie."""
+    d, om, sg, arr = (log[:, k] for k in range(4))
+    with np.errstate(invalid="ignore", divide="ignore"):
+        def rel(x, y):
+            den = np.maximum(np.abs(x), np.abs(y))
+            return np.where(den > 0, np.abs(x - y) / np.where(den > 0, den, 1.0), np.inf)
+        m = rel(d, ALPHA * om)
+        m = np.where(om == 0.0, np.inf, m)
+        cand = ~np.isnan(sg)
+        m2 = rel(d * sg, ALPHA * om * om)
+        m3 = rel(arr, ALPHA * sg)
+        m = np.where(cand, np.minimum(m, np.minimum(m2, m3)), m)
+        return np.where(np.isnan(d), np.nan, m)
 
 
 def factor_workspace_size(n: int, block_size: int) -> int:

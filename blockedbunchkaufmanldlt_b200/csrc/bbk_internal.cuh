@@ -218,6 +218,7 @@ struct DeviceState {
 // parity): no CTA can be two exchanges ahead of another.
 // ---------------------------------------------------------------------------
 constexpr int kSlotWords = 32;   // words per CTA record
+constexpr int kPivLogWords = 4;  // decision log: |W(p,p)|, omega, sigma, |W(r,r)|
 constexpr int kMaxPub = 10;      // published doubles per record
 
 __device__ __forceinline__ unsigned long long tag_word(unsigned tag, unsigned v) {
@@ -252,6 +253,14 @@ int solve_enqueue(int n, const double* f, long long ldf, const int* perm,
                   const int* pivot_types, int nrhs, double* b, long long ldb,
                   double* work, cudaStream_t s);
 size_t solve_work_doubles(int n, int nrhs);
+// The status word solve_enqueue keeps inside its scratch (BBK_OK, or
+// BBK_ERR_TIMEOUT when a sweep's bounded wait ran out), and a synchronous
+// read of it after the solve (waits for the stream).
+int* solve_status_word(double* work, int n, int nrhs);
+int solve_status(double* work, int n, int nrhs, cudaStream_t s);
+// solve_enqueue under the library's per-kernel-class timing (capi.cu).
+int enqueue_solve(int n, const double* f, long long ldf, const int* perm, const int* pt,
+                  int nrhs, double* b, long long ldb, double* work, cudaStream_t s);
 size_t refine_work_doubles(int n, int nrhs, int restart);
 int refine_enqueue(int n, const double* a, long long lda, const double* f, long long ldf,
                    const int* perm, const int* pt, int nrhs, const double* b, double* x, double tol,
@@ -296,5 +305,6 @@ struct FactorPlan {
   void* hsplit = nullptr;    // BF16 update: 2 operands x 3 terms x hstride BF16, split once per panel
   int kpad = 0;              // BF16 update: panel width rounded up to 32 (k pitch of hsplit)
   size_t hstride = 0;        // BF16 update: elements per operand term (n_pad x kpad)
+  double* pivlog = nullptr;  // optional decision log (kPivLogWords doubles per position)
 };
 }  // namespace bbk

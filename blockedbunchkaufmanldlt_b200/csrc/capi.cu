@@ -70,7 +70,9 @@ struct Carver {
 // Lays out (or, with base == nullptr, measures) the factorization workspace.
 size_t carve_factor(FactorPlan& plan, char* base) {
   const int n = plan.n, b = plan.b;
-  const long long npad = static_cast<long long>(align_up(static_cast<size_t>(n), 64));
+  // 128-aligned: the update's 128 x 128 tiles read W columns and U rows up
+  // to the next multiple of 128
+  const long long npad = static_cast<long long>(align_up(static_cast<size_t>(n), 128));
   plan.ldw = npad;
   plan.ldu = static_cast<int>(align_up(static_cast<size_t>(b) + 2, 4));
   Carver c{base};
@@ -202,8 +204,8 @@ static int enqueue_factor(FactorPlan& plan, int* status_device, cudaStream_t s) 
   return launch_status_copy(plan.state, status_device, s);
 }
 
-static int enqueue_solve(int n, const double* f, long long ldf, const int* perm, const int* pt,
-                         int nrhs, double* b, long long ldb, double* work, cudaStream_t s) {
+int enqueue_solve(int n, const double* f, long long ldf, const int* perm, const int* pt,
+                  int nrhs, double* b, long long ldb, double* work, cudaStream_t s) {
   return profiled(kProfSolve, s, [&] {
     return solve_enqueue(n, f, ldf, perm, pt, nrhs, b, ldb, work, s);
   });
@@ -312,9 +314,10 @@ size_t bbk_factor_workspace_size(int n, int block_size) {
   return carve_factor(plan, nullptr);
 }
 
-int bbk_factor_device_async(int n, int block_size, double* a, long long lda, int* perm,
-                            int* pivot_types, int* panel_end, int update_mode, void* workspace,
-                            size_t workspace_bytes, int* status_device, void* stream) {
+static int factor_async(int n, int block_size, double* a, long long lda, int* perm,
+                        int* pivot_types, int* panel_end, int update_mode, double* pivot_log,
+                        void* workspace, size_t workspace_bytes, int* status_device,
+                        void* stream) {
   int rc = validate_factor_args(n, block_size, a, lda, perm, pivot_types, update_mode);
   if (rc) return rc;
   if ((rc = check_device())) return rc;
@@ -335,6 +338,11 @@ int bbk_factor_device_async(int n, int block_size, double* a, long long lda, int
   plan.grid = panel_grid_size(n);
   plan.timeout_ns = wait_timeout_ns();
   plan.stats = g_panel_stats_on ? g_panel_stats : nullptr;
+  plan.pivlog = pivot_log;
+  if (pivot_log) {
+    // all-ones bytes: NaN at every position no decision writes
+    BBK_CUDA_TRY(cudaMemsetAsync(pivot_log, 0xff, static_cast<size_t>(n) * kPivLogWords * sizeof(double), s));
+  }
   const size_t need = carve_factor(plan, nullptr);
   char* base = static_cast<char*>(workspace);
   bool owned = false;
@@ -358,6 +366,22 @@ int bbk_factor_device_async(int n, int block_size, double* a, long long lda, int
     if (!rc && err != cudaSuccess) rc = cuda_error(err, "cudaFreeAsync");
   }
   return rc;
+}
+
+int bbk_factor_device_async(int n, int block_size, double* a, long long lda, int* perm,
+                            int* pivot_types, int* panel_end, int update_mode, void* workspace,
+                            size_t workspace_bytes, int* status_device, void* stream) {
+  return factor_async(n, block_size, a, lda, perm, pivot_types, panel_end, update_mode, nullptr,
+                      workspace, workspace_bytes, status_device, stream);
+}
+
+int bbk_factor_device_logged(int n, int block_size, double* a, long long lda, int* perm,
+                             int* pivot_types, int* panel_end, int update_mode,
+                             double* pivot_log, void* workspace, size_t workspace_bytes,
+                             int* status_device, void* stream) {
+  if (pivot_log == nullptr) return set_error(BBK_ERR_INVALID_ARGUMENT, "null pivot log");
+  return factor_async(n, block_size, a, lda, perm, pivot_types, panel_end, update_mode, pivot_log,
+                      workspace, workspace_bytes, status_device, stream);
 }
 
 int bbk_factor_device(int n, int block_size, double* a, long long lda, int* perm,
@@ -425,10 +449,9 @@ int bbk_solve_device(int n, const double* factors, long long ldf, const int* per
                      workspace_bytes);
   }
   rc = enqueue_solve(n, factors, ldf, perm, pivot_types, nrhs, b, ldb, work, s);
+  if (!rc) rc = solve_status(work, n, nrhs, s);  // waits for the solve
   if (owned) cudaFreeAsync(work, s);
-  if (rc) return rc;
-  BBK_CUDA_TRY(cudaStreamSynchronize(s));
-  return BBK_OK;
+  return rc;
 }
 
 int bbk_solve_host(int n, const double* factors, long long ldf, const int* perm,
@@ -457,6 +480,7 @@ int bbk_solve_host(int n, const double* factors, long long ldf, const int* perm,
     rc = cuda_error(err, "solve setup");
   } else {
     rc = enqueue_solve(n, d_f, ldf, d_perm, d_pt, nrhs, d_b, ldb, work, s);
+    if (!rc) rc = solve_status(work, n, nrhs, s);
     if (!rc) {
       err = cudaMemcpyAsync(b, d_b, bbytes, cudaMemcpyDeviceToHost, s);
       if (err == cudaSuccess) err = cudaStreamSynchronize(s);
@@ -518,8 +542,12 @@ int bbk_factor_solve_host(int n, int block_size, double* a, long long lda, int* 
       if (err == cudaSuccess) err = cudaEventRecord(factored, s);
       if (err != cudaSuccess) rc = cuda_error(err, "factorization copy stream");
     }
-    if (!rc && nrhs > 0) rc = enqueue_solve(n, d_a, lda, d_perm, d_pt, nrhs, d_b, ldb,
-                                            reinterpret_cast<double*>(ws), s);
+    int* solve_st = nullptr;
+    int h_solve = BBK_OK;
+    if (!rc && nrhs > 0) {
+      rc = enqueue_solve(n, d_a, lda, d_perm, d_pt, nrhs, d_b, ldb, reinterpret_cast<double*>(ws), s);
+      solve_st = solve_status_word(reinterpret_cast<double*>(ws), n, nrhs);
+    }
     if (!rc) {
       // the second stream's copies are enqueued first: a copy into pageable
       // memory (the status word below, or a caller's pageable buffer) can
@@ -532,9 +560,13 @@ int bbk_factor_solve_host(int n, int block_size, double* a, long long lda, int* 
         err = cudaMemcpyAsync(panel_end, d_pe, nb * sizeof(int), cudaMemcpyDeviceToHost, s2);
       if (err == cudaSuccess && nrhs > 0) err = cudaMemcpyAsync(b, d_b, bbytes, cudaMemcpyDeviceToHost, s);
       if (err == cudaSuccess) err = cudaMemcpyAsync(&h_status, d_status, sizeof(int), cudaMemcpyDeviceToHost, s);
+      if (err == cudaSuccess && solve_st)
+        err = cudaMemcpyAsync(&h_solve, solve_st, sizeof(int), cudaMemcpyDeviceToHost, s);
       if (err == cudaSuccess) err = cudaStreamSynchronize(s2);
       if (err == cudaSuccess) err = cudaStreamSynchronize(s);
       if (err != cudaSuccess) rc = cuda_error(err, "factorization");
+      if (!rc && h_status == BBK_OK && h_solve != BBK_OK)
+        rc = set_error(h_solve, "solve aborted on the device: %s", bbk_status_string(h_solve));
     }
     if (s2) {
       // the frees below are ordered on s: s waits for s2's copies first
@@ -611,8 +643,9 @@ int bbk_solve_refined_device(int n, const double* a, long long lda, const double
   } else {
     // x0 from the factors, then FP64 refinement (the solve scratch sits at
     // the end of the refinement workspace)
-    rc = enqueue_solve(n, factors, ldf, perm, pivot_types, nrhs, xc, n,
-                       work + refine_work_doubles(n, nrhs, m) - solve_work_doubles(n, nrhs), s);
+    double* swork = work + refine_work_doubles(n, nrhs, m) - solve_work_doubles(n, nrhs);
+    rc = enqueue_solve(n, factors, ldf, perm, pivot_types, nrhs, xc, n, swork, s);
+    if (!rc) rc = solve_status(swork, n, nrhs, s);
     if (!rc)
       rc = refine_enqueue(n, a, lda, factors, ldf, perm, pivot_types, nrhs, bc, xc, tol, max_iter,
                           method, m, work, info, s);

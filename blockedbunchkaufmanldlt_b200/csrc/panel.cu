@@ -98,6 +98,7 @@ struct PanelArgs {
   int smem_cols;     // slice width the shared-memory allocation holds
   unsigned long long* stats;  // optional per-phase nanoseconds (CTA 0)
   unsigned poll_ns;           // pause between polls of the arrival counter
+  double* pivlog;             // optional decision log, kPivLogWords per position
 };
 
 __device__ __forceinline__ void fail(DeviceState* st, int code) {
@@ -603,6 +604,8 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
 
     int kind = 1;  // 1: 1x1 at p; -1: 1x1 after p<->r; 2: 2x2 with p+1<->r
     bool cand = false, spec = false;
+    double log_sigma = __longlong_as_double(0x7ff8000000000000ll);  // NaN: no candidate
+    double log_arr = log_sigma;
     double wc_r = 0.0, wc_p = 0.0, wc_p1 = 0.0, wc_p2 = 0.0;
     double nx_ar = 0.0, nx_part = 0.0, nx_d = 0.0, nx_1 = 0.0, nx_2 = 0.0;
     double e0 = 0.0;  // U[p, p+1] when p stays a 1x1 pivot (row computed ahead)
@@ -784,6 +787,8 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
         nx_part = X.pub[8];
       }
       lap(3);
+      log_sigma = sigma;
+      log_arr = fabs(wc_r);
       // SelectPivot, :369-390
       if (xsub(xmul(fabs(dpp), sigma), xmul(xmul(kAlpha, omega), omega)) >= 0.0) {
         kind = 1;
@@ -795,6 +800,15 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
       // :104-108: a 2x2 pivot starting at the panel's last column moves that
       // column into the next panel (ShiftBoundaryColumnToNextBlock).
       if (kind == 2 && p == P.nominal_end - 1 && P.can_shift) break;
+    }
+    if (P.pivlog != nullptr && c == 0 && t == 0) {
+      // the quantities this step's decision compared (FactorPanel :90-92,
+      // SelectPivot :369-390), at the position where its pivot starts
+      double* lg = P.pivlog + static_cast<size_t>(p) * kPivLogWords;
+      lg[0] = fabs(dpp);
+      lg[1] = omega;
+      lg[2] = log_sigma;
+      lg[3] = log_arr;
     }
 
     if (kind == 1) {
@@ -1233,6 +1247,7 @@ int launch_panel(const FactorPlan& plan, int panel, cudaStream_t s) {
   P.slot_stride = plan.grid;
   P.timeout_ns = plan.timeout_ns;
   P.stats = plan.stats;
+  P.pivlog = plan.pivlog;
   static const unsigned poll_ns = [] {
     const char* e = getenv("BBK_POLL_NS");
     return e ? static_cast<unsigned>(atoi(e)) : 0u;

@@ -188,7 +188,10 @@ struct Refiner {
     return BBK_OK;
   }
   int precond(int nv, double* v) {  // v <- (LDL^T)^{-1} v in place
-    return solve_enqueue(n, f, ldf, perm, pt, nv, v, n, solve_work, s);
+    const int rc = enqueue_solve(n, f, ldf, perm, pt, nv, v, n, solve_work, s);
+    // the next solve resets the status word: read it now (the loop waits
+    // for the stream after each preconditioner application anyway)
+    return rc ? rc : solve_status(solve_work, n, nv, s);
   }
 };
 

@@ -14,6 +14,7 @@
 // publishes it with a release flag.  Only the newest block's contribution and
 // the triangle are on the critical path; the factor is read once per sweep.
 #include <algorithm>
+#include <mutex>
 
 #include "bbk_internal.cuh"
 
@@ -321,6 +322,9 @@ __global__ void rec_kernel(int n, const double* f, long long ldf, const int* pt,
   out[static_cast<long long>(perm[i]) * ldo + perm[j]] = s;
 }
 
+constexpr int kMaxAttrDevices = 64;
+std::once_flag g_sweep_attr[kMaxAttrDevices];
+
 int grid_for(long long work, int threads) {
   const long long g = (work + threads - 1) / threads;
   return static_cast<int>(std::max(1LL, std::min(g, 4096LL)));
@@ -330,6 +334,19 @@ int grid_for(long long work, int threads) {
 
 size_t solve_work_doubles(int n, int nrhs) { return 2 * static_cast<size_t>(n) * nrhs; }
 
+int* solve_status_word(double* work, int n, int nrhs) {
+  const int nblk = (n + kSB - 1) / kSB;
+  return reinterpret_cast<int*>(work + static_cast<long long>(n) * nrhs) + nblk;
+}
+
+int solve_status(double* work, int n, int nrhs, cudaStream_t s) {
+  int h = BBK_OK;
+  BBK_CUDA_TRY(cudaMemcpyAsync(&h, solve_status_word(work, n, nrhs), sizeof(int), cudaMemcpyDeviceToHost, s));
+  BBK_CUDA_TRY(cudaStreamSynchronize(s));
+  if (h != BBK_OK) return set_error(h, "solve aborted on the device: %s", bbk_status_string(h));
+  return BBK_OK;
+}
+
 // work: 2 n nrhs doubles: the right-hand sides being solved in place, then
 // the block flags and the status word.
 int solve_enqueue(int n, const double* f, long long ldf, const int* perm, const int* pivot_types,
@@ -338,7 +355,7 @@ int solve_enqueue(int n, const double* f, long long ldf, const int* perm, const 
   const long long total = static_cast<long long>(n) * nrhs;
   const int nblk = (n + kSB - 1) / kSB;
   int* flags = reinterpret_cast<int*>(work + total);
-  int* status = flags + nblk;
+  int* status = solve_status_word(work, n, nrhs);
   reset_flags_kernel<<<std::max(1, std::min(64, (nblk + 256) / 256)), 256, 0, s>>>(flags, nblk + 1);
   BBK_CUDA_TRY(cudaGetLastError());
   count_launch();
@@ -346,17 +363,21 @@ int solve_enqueue(int n, const double* f, long long ldf, const int* perm, const 
   BBK_CUDA_TRY(cudaGetLastError());
   count_launch();
   SweepArgs A{n, nrhs, f, ldf, pivot_types, y, flags, status, 1, wait_timeout_ns()};
-  static bool attr_set[64] = {};
+  // 53 KB of dynamic shared memory exceeds the default 48 KB; the attribute
+  // is set per device, each under its own once-flag (callers may be on
+  // several host threads)
   int dev = 0;
   BBK_CUDA_TRY(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 64 || !attr_set[dev]) {
-    // 53 KB of dynamic shared memory exceeds the default 48 KB
-    BBK_CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void*>(psweep_kernel<true>),
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSweepSmem)));
-    BBK_CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void*>(psweep_kernel<false>),
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSweepSmem)));
-    if (dev >= 0 && dev < 64) attr_set[dev] = true;
-  }
+  if (dev < 0 || dev >= kMaxAttrDevices) return set_error(BBK_ERR_NO_DEVICE, "device %d out of range", dev);
+  cudaError_t attr_err = cudaSuccess;
+  std::call_once(g_sweep_attr[dev], [&] {
+    attr_err = cudaFuncSetAttribute(reinterpret_cast<const void*>(psweep_kernel<true>),
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSweepSmem));
+    if (attr_err == cudaSuccess)
+      attr_err = cudaFuncSetAttribute(reinterpret_cast<const void*>(psweep_kernel<false>),
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSweepSmem));
+  });
+  BBK_CUDA_TRY(attr_err);
   const int grid = std::max(1, std::min(nblk, device_sm_count()));
   {
     void* kargs[] = {&A};

@@ -10,11 +10,13 @@
 //
 // The array is a file-scope __device__ variable: every GPU that loads the
 // library holds its 8 MiB until the process exits.  In host code its name is
-// only a host-side stand-in, so the device address is looked up with
-// cudaGetSymbolAddress once per device (with that device current) and only
-// that address is ever handed to kernels.
-#include <mutex>
-
+// only a host-side stand-in, so on every call the device address is looked
+// up with cudaGetSymbolAddress (with the call's device current) and only
+// that address is handed to kernels.  The lookup is not cached: after a
+// cudaDeviceReset, or in another context on the same device, the library's
+// module is loaded again and the array can sit elsewhere.  The first lookup
+// on a device may load the module, so the first call should come before any
+// stream capture.
 #include "bbk_internal.cuh"
 
 namespace bbk {
@@ -22,26 +24,17 @@ namespace {
 
 constexpr long long kNoAllocMaxElements = BBK_SOLVE_NOALLOC_MAX_ELEMENTS;  // n * nrhs
 
-// Two ping-pong copies of the right-hand sides (see solve_enqueue).
+// The solve's scratch, laid out as solve_enqueue uses it: the right-hand
+// sides being solved (n * nrhs doubles), then one flag per 64-row block and
+// the status word.  Sized like solve_work_doubles(n, nrhs) at the limit.
 static __device__ __align__(256) double g_solve_scratch[2 * kNoAllocMaxElements];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_scratch_mu;
-double* g_scratch_addr[kMaxDevices] = {nullptr};
-
-// Device address of g_solve_scratch on the current device (looked up once).
+// Device address of g_solve_scratch in the current context.
 int scratch_address(double** out) {
-  int dev = 0;
-  BBK_CUDA_TRY(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kMaxDevices) return set_error(BBK_ERR_NO_DEVICE, "device %d out of range", dev);
-  std::lock_guard<std::mutex> lk(g_scratch_mu);
-  if (g_scratch_addr[dev] == nullptr) {
-    void* p = nullptr;
-    const cudaError_t err = cudaGetSymbolAddress(&p, g_solve_scratch);
-    if (err != cudaSuccess) return cuda_error(err, "cudaGetSymbolAddress(solve scratch)");
-    g_scratch_addr[dev] = static_cast<double*>(p);
-  }
-  *out = g_scratch_addr[dev];
+  void* p = nullptr;
+  const cudaError_t err = cudaGetSymbolAddress(&p, g_solve_scratch);
+  if (err != cudaSuccess) return cuda_error(err, "cudaGetSymbolAddress(solve scratch)");
+  *out = static_cast<double*>(p);
   return BBK_OK;
 }
 
@@ -74,8 +67,9 @@ extern "C" int bbk_solve_device_noalloc(int n, const double* factors, long long 
   double* scratch = nullptr;
   int rc = scratch_address(&scratch);
   if (rc) return rc;
-  // Every element of the scratch is written before it is read, so the
-  // previous call's contents need no clearing.
-  return solve_enqueue(n, factors, ldf, perm, pivot_types, nrhs, b, ldb, scratch,
+  // Every element of the scratch is written before it is read (the block
+  // flags and the status word are cleared by the solve's first kernel), so
+  // the previous call's contents need no clearing.
+  return enqueue_solve(n, factors, ldf, perm, pivot_types, nrhs, b, ldb, scratch,
                        static_cast<cudaStream_t>(stream));
 }

@@ -24,6 +24,7 @@
 
 #include <algorithm>
 #include <cstdlib>
+#include <mutex>
 #include <type_traits>
 
 #include "bbk_internal.cuh"
@@ -454,6 +455,184 @@ __global__ void __launch_bounds__(kThreadsMma) mma_update_kernel(UpdArgs U) {
 }
 
 // ---------------------------------------------------------------------------
+// FP64 tensor-core update with 128x128 C tiles (the large trailing matrices).
+// 8 warps of 64x32, k chunks of 32 in a kStagesL-deep cp.async ring that
+// runs across tile boundaries (the next tile's first chunks load while this
+// tile finishes), so the tensor pipe only waits at an epilogue.  Each C tile
+// is prefetched into L2 when its first chunk is consumed and updated straight
+// from registers (C -= acc) at its end.  Against the 64x64 tile this halves
+// the L2 operand traffic per flop (each A/B element feeds 128 instead of 64
+// outputs) and the C traffic per flop stays the same.
+// ---------------------------------------------------------------------------
+constexpr int kBML = 128, kBNL = 128;
+constexpr int kThreadsL = 256;
+constexpr int kStagesL = 3;
+constexpr int kAPitchL = kBK + kPadA;   // A stage [128][36]: k contiguous
+constexpr int kBPitchL = kBNL + kPadB;  // B stage [32][132]: j contiguous
+constexpr int kAStageL = kBML * kAPitchL;
+constexpr int kStageL = kAStageL + kBK * kBPitchL;
+constexpr size_t kBytesL = static_cast<size_t>(kStagesL) * kStageL * sizeof(double);
+static_assert(kBytesL <= 227 * 1024, "stages must fit the shared memory of one CTA");
+
+__device__ __forceinline__ int tile_count_l(int tm) { return tm * (tm + 1) / 2; }
+
+// Chunk ch of tile (i0, j0) into stage st: A 128 x 32, B 32 x 128, 16-byte
+// copies (k >= inner zero-filled).
+__device__ __forceinline__ void load_stage_l(const UpdArgs& U, double* st, int i0, int j0, int k0) {
+  double* as = st;
+  double* bs = st + kAStageL;
+  const int t = threadIdx.x;
+#pragma unroll
+  for (int u = 0; u < (kBML * kBK / 2) / kThreadsL; ++u) {
+    const int c = t + u * kThreadsL;
+    const int ii = c / (kBK / 2), kk = (c % (kBK / 2)) * 2;
+    const int k = k0 + kk;
+    const int nvalid = max(0, min(2, U.inner - k));
+    const double* src = U.a + static_cast<long long>(i0 + ii) * U.a_si + (nvalid ? k : 0);
+    cp_async_16(&as[ii * kAPitchL + kk], src, nvalid * 8);
+  }
+#pragma unroll
+  for (int u = 0; u < (kBK * kBNL / 2) / kThreadsL; ++u) {
+    const int c = t + u * kThreadsL;
+    const int kk = c / (kBNL / 2), jj = (c % (kBNL / 2)) * 2;
+    const int k = k0 + kk;
+    const bool ok = k < U.inner;
+    const double* src = U.b + static_cast<long long>(ok ? k : 0) * U.b_sk + j0 + jj;
+    cp_async_16(&bs[kk * kBPitchL + jj], src, ok ? 16 : 0);
+  }
+}
+
+__device__ __forceinline__ void tile_origin_l(const UpdArgs& U, int t, int& i0, int& j0) {
+  int j = static_cast<int>((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+  while (j * (j + 1) / 2 > t) --j;
+  while ((j + 1) * (j + 2) / 2 <= t) ++j;
+  i0 = U.tile_i0 + (t - j * (j + 1) / 2) * kBML;
+  j0 = U.tile_i0 + j * kBNL;
+}
+
+__global__ void __launch_bounds__(kThreadsL, 1) mma_update_large_kernel(UpdArgs U) {
+  extern __shared__ double smem[];
+  if (U.st != nullptr) {
+    // panel mode: range from the device state, tiles of 128 from the
+    // 128-aligned row at or below the trailing matrix's first row
+    if (ld_relaxed_s32(&U.st->abort)) return;
+    const int k0 = ldcg(&U.st->kstart[U.panel & 1]);
+    const int e = ldcg(&U.st->kstart[(U.panel + 1) & 1]);
+    U.inner = e - k0;
+    U.i_lo = U.j_lo = e;
+    U.i_hi = U.j_hi = U.n;
+    U.tile_i0 = U.tile_j0 = (e / kBML) * kBML;
+    if (U.inner <= 0 || e >= U.n) return;
+  }
+  const int tm = (U.n - U.tile_i0 + kBML - 1) / kBML;
+  const int ntiles = tile_count_l(tm);
+  if (static_cast<int>(blockIdx.x) >= ntiles) return;
+  const int nchunks = (U.inner + kBK - 1) / kBK;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, tq = lane & 3;
+  const int wm = (warp >> 2) * 64, wn = (warp & 3) * 32;
+  // (tile, chunk) items of this CTA, in order: tiles blockIdx.x + m * gridDim.x
+  const int my_tiles = (ntiles - static_cast<int>(blockIdx.x) + static_cast<int>(gridDim.x) - 1) /
+                       static_cast<int>(gridDim.x);
+  const long long items = static_cast<long long>(my_tiles) * nchunks;
+  // loader cursor (item ld_item = tile ld_tile, chunk ld_ch)
+  long long ld_item = 0;
+  int ld_ch = 0, ld_m = 0, ld_i0 = 0, ld_j0 = 0;
+  tile_origin_l(U, blockIdx.x, ld_i0, ld_j0);
+  auto issue = [&]() {
+    if (ld_item < items) {
+      load_stage_l(U, smem + static_cast<size_t>(ld_item % kStagesL) * kStageL, ld_i0, ld_j0, ld_ch * kBK);
+      ++ld_item;
+      if (++ld_ch == nchunks) {
+        ld_ch = 0;
+        ++ld_m;
+        if (ld_m < my_tiles)
+          tile_origin_l(U, static_cast<int>(blockIdx.x) + ld_m * static_cast<int>(gridDim.x), ld_i0, ld_j0);
+      }
+    }
+    cp_async_commit();  // one group per item slot, empty past the end
+  };
+#pragma unroll
+  for (int s = 0; s < kStagesL - 1; ++s) issue();
+
+  long long item = 0;
+  for (int m = 0; m < my_tiles; ++m) {
+    int i0, j0;
+    tile_origin_l(U, static_cast<int>(blockIdx.x) + m * static_cast<int>(gridDim.x), i0, j0);
+    // the C tile's rows go to L2 now; the epilogue reads them after the k loop
+    for (int r = threadIdx.x >> 3; r < kBML; r += kThreadsL / 8) {
+      const int i = i0 + r;
+      const int jc = j0 + (threadIdx.x & 7) * 16;
+      if (i >= U.i_lo && i < U.i_hi && jc < U.j_hi && i <= jc + 15)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(U.c + static_cast<long long>(i) * U.ldc + jc));
+    }
+    double acc[4][4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.0;
+    for (int ch = 0; ch < nchunks; ++ch, ++item) {
+      cp_async_wait<kStagesL - 2>();
+      __syncthreads();  // item's stage has landed; every warp is done with the stage refilled next
+      issue();
+      const double* as = smem + static_cast<size_t>(item % kStagesL) * kStageL;
+      const double* bs = as + kAStageL;
+#pragma unroll
+      for (int ks = 0; ks < kBK; ks += 8) {
+        double af[4][4], bf[4][2];
+#pragma unroll
+        for (int mt = 0; mt < 4; ++mt) {
+          const int r = wm + mt * 16 + g;
+          af[mt][0] = as[r * kAPitchL + ks + tq];
+          af[mt][1] = as[(r + 8) * kAPitchL + ks + tq];
+          af[mt][2] = as[r * kAPitchL + ks + tq + 4];
+          af[mt][3] = as[(r + 8) * kAPitchL + ks + tq + 4];
+        }
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+          const int col = wn + nt * 8 + g;
+          bf[nt][0] = bs[(ks + tq) * kBPitchL + col];
+          bf[nt][1] = bs[(ks + tq + 4) * kBPitchL + col];
+        }
+#pragma unroll
+        for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+          for (int nt = 0; nt < 4; ++nt) mma_16x8x8(acc[mt][nt], af[mt], bf[nt]);
+      }
+    }
+    // C -= acc on the tile's valid part (upper triangle of the trailing matrix)
+#pragma unroll
+    for (int mt = 0; mt < 4; ++mt) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int i = i0 + wm + mt * 16 + g + h * 8;
+        if (i < U.i_lo || i >= U.i_hi) continue;
+        double* crow = U.c + static_cast<long long>(i) * U.ldc;
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+          const int j = j0 + wn + nt * 8 + tq * 2;
+          const double v0 = acc[mt][nt][h * 2], v1 = acc[mt][nt][h * 2 + 1];
+          const bool ok0 = j >= U.j_lo && j < U.j_hi && (!U.upper_only || i <= j);
+          const bool ok1 = j + 1 >= U.j_lo && j + 1 < U.j_hi && (!U.upper_only || i <= j + 1);
+          if (ok0 && ok1) {
+            double2 cv = *reinterpret_cast<const double2*>(crow + j);
+            cv.x -= v0;
+            cv.y -= v1;
+            *reinterpret_cast<double2*>(crow + j) = cv;
+          } else {
+            if (ok0) crow[j] -= v0;
+            if (ok1) crow[j + 1] -= v1;
+          }
+        }
+      }
+    }
+  }
+  cp_async_wait<0>();
+}
+
+// ---------------------------------------------------------------------------
 // SIMT tiles: reference-ordered FP64 and FP32.  256 threads, 4x4 per thread.
 // ---------------------------------------------------------------------------
 constexpr int kThreadsSimt = 256;
@@ -541,6 +720,16 @@ bool use_k16() {
   static const bool v = [] {
     const char* e = getenv("BBK_UPDATE_K16");
     return e ? atoi(e) != 0 : false;
+  }();
+  return v;
+}
+
+// 128x128 tiles for large trailing matrices (BBK_UPDATE_LARGE_TILES=0
+// keeps the 64x64 kernel everywhere: tuning and comparison).
+bool use_large_tiles() {
+  static const bool v = [] {
+    const char* e = getenv("BBK_UPDATE_LARGE_TILES");
+    return e ? atoi(e) != 0 : true;
   }();
   return v;
 }
@@ -945,6 +1134,29 @@ int launch_update(const FactorPlan& plan, int panel, cudaStream_t s) {
     return plan.mode == BBK_UPDATE_BF16
                ? launch_bf16_split<1>(U, buf, plan.kpad, plan.hstride, grid_mma, vec, s)
                : launch_bf16_split<3>(U, buf, plan.kpad, plan.hstride, grid_mma, vec, s);
+  }
+  if (plan.mode == BBK_UPDATE_FP64 && vec && use_large_tiles()) {
+    // 128x128 tiles while the trailing matrix gives every SM at least two of
+    // them (the grid is persistent, one CTA per SM)
+    const long long tml = (plan.n - (nominal_e / kBML) * kBML + kBML - 1) / kBML;
+    const long long tiles_l = tml * (tml + 1) / 2;
+    if (tiles_l >= 2LL * sms) {
+      static std::once_flag attr_once[64];
+      int dev = 0;
+      BBK_CUDA_TRY(cudaGetDevice(&dev));
+      if (dev < 0 || dev >= 64) return set_error(BBK_ERR_NO_DEVICE, "device %d out of range", dev);
+      cudaError_t attr_err = cudaSuccess;
+      std::call_once(attr_once[dev], [&] {
+        attr_err = cudaFuncSetAttribute(mma_update_large_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(kBytesL));
+      });
+      BBK_CUDA_TRY(attr_err);
+      const int grid = static_cast<int>(std::min<long long>(tiles_l, sms));
+      mma_update_large_kernel<<<grid, kThreadsL, kBytesL, s>>>(U);
+      BBK_CUDA_TRY(cudaGetLastError());
+      count_launch();
+      return BBK_OK;
+    }
   }
   return launch_by_mode(U, plan.mode, true, vec, grid_mma, grid_simt, s);
 }

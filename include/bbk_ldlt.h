@@ -133,6 +133,22 @@ int bbk_factor_device_async(int n, int block_size, double* a, long long lda,
                             int update_mode, void* workspace,
                             size_t workspace_bytes, int* status_device,
                             void* stream);
+/* Diagnostics for pivot-sequence comparisons: bbk_factor_device_async that
+ * also records what every Bunch-Kaufman decision compared, so a decision
+ * that another summation order could flip (a near-tie) can be recognised.
+ * pivot_log (device, 4 * n doubles) receives, at the factored position p
+ * where each pivot step's pivot starts: |W(p,p)| (tested against alpha *
+ * omega, src/block_ldlt_decomposition.cc:90-92), omega = max_{j>p} |W(p,j)|
+ * (FindCurrentRowMax, :164-182), sigma = max_{i>=p, i!=r} |W(i,r)| and
+ * |W(r,r)| (FindCandidateColumnMax and SelectPivot, :354-390; NaN when the
+ * first test kept the 1x1 pivot).  Every other entry is NaN (the second row
+ * of a 2x2 pivot).  The reference has no such log; the bench and the parity
+ * tests use it. */
+int bbk_factor_device_logged(int n, int block_size, double* a, long long lda,
+                             int* perm, int* pivot_types, int* panel_end,
+                             int update_mode, double* pivot_log,
+                             void* workspace, size_t workspace_bytes,
+                             int* status_device, void* stream);
 /* Host variant: a (n x lda, in/out), perm, pivot_types, panel_end are host
  * memory.  Copies in, factors on the current device, copies out. */
 int bbk_factor_host(int n, int block_size, double* a, long long lda,
@@ -164,13 +180,17 @@ int bbk_solve_host(int n, const double* factors, long long ldf,
  * library that every GPU loading the library holds until the process exits,
  * so n * nrhs may be at most BBK_SOLVE_NOALLOC_MAX_ELEMENTS (larger sizes are
  * rejected with BBK_ERR_INVALID_ARGUMENT).  The first call on each device
- * looks up that array's device address; make that first call before any
- * stream capture.  All calls on a device share the array and it keeps the
- * last call's contents (nothing in it needs clearing: every element is
- * written before it is read), so calls whose work overlaps on the GPU --
- * different streams, or different host threads -- race and corrupt each
- * other.  Enqueues on `stream` and returns without waiting; device
- * pointers. */
+ * may load the library's device code to find that array's address; make
+ * that first call before any stream capture.  All calls on a device share
+ * the array and it keeps the last call's contents (nothing in it needs
+ * clearing: every element is written before it is read), so calls whose
+ * work overlaps on the GPU -- different streams, or different host threads
+ * -- race and corrupt each other.  Enqueues on `stream` and returns without
+ * waiting; device pointers.  Because it returns before the solve runs, it
+ * cannot report a solve whose device-side bounded wait ran out (the
+ * synchronous bbk_solve_device returns BBK_ERR_TIMEOUT for that); the
+ * sweeps' waits only run out if the GPU cannot keep their blocks resident
+ * together, and the right-hand sides are then left partly solved. */
 #define BBK_SOLVE_NOALLOC_MAX_ELEMENTS 524288
 int bbk_solve_device_noalloc(int n, const double* factors, long long ldf,
                              const int* perm, const int* pivot_types,

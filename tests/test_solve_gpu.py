@@ -58,3 +58,25 @@ def test_zero_pivot_gives_zero_component(cuda, bbk, port):
     x = bbk.solve_host(fac, rhs)
     assert np.allclose(x, port.solve(port.factor(a, 2), rhs))
     assert x[2] == 0.0
+
+
+def test_solve_reports_an_expired_wait_and_the_context_survives(cuda, bbk):
+    # With a 1 ns bound every sweep block that has to wait for an earlier one
+    # gives up (n = 4096: 64 blocks, most of them wait): the synchronous solve
+    # must return BBK_ERR_TIMEOUT instead of partly solved right-hand sides
+    # with BBK_OK, and the next solve with the normal bound must succeed.
+    import torch
+    n, blk = 4096, 64
+    a = uniform_symmetric(n, 4096)
+    f = torch.from_numpy(a).to(cuda)
+    perm, pt, _ = bbk.factor_device(f, blk)
+    rhs = np.random.default_rng(7).standard_normal((2, n))
+    try:
+        bbk.set_wait_timeout_ns(1)
+        with pytest.raises(bbk.BbkError) as err:
+            bbk.solve_device(f, perm, pt, torch.from_numpy(rhs).to(cuda))
+        assert err.value.status == bbk.BBK_ERR_TIMEOUT
+    finally:
+        bbk.set_wait_timeout_ns(5_000_000_000)
+    x = bbk.solve_device(f, perm, pt, torch.from_numpy(rhs).to(cuda)).cpu().numpy()
+    assert backward_error(a, x.T, rhs.T) < 1e-14

@@ -40,6 +40,9 @@ def _solve_noalloc(bbk, f, perm, pt, b):
 
 
 def test_noalloc_matches_existing_solve_twice(cuda, bbk):
+    # Both entry points run the same kernels on the same data, so the
+    # results must be identical bit for bit (a stale or overlapping scratch
+    # would show as a difference).
     import torch
     n, blk = 1500, 64
     f = torch.from_numpy(uniform_symmetric(n, 99)).to(cuda)
@@ -49,7 +52,29 @@ def test_noalloc_matches_existing_solve_twice(cuda, bbk):
         b = torch.from_numpy(rng.standard_normal((nrhs, n))).to(cuda)
         want = _solve_existing(bbk, f, perm, pt, b).cpu().numpy()
         got = _solve_noalloc(bbk, f, perm, pt, b).cpu().numpy()
-        assert np.max(np.abs(got - want)) <= 1e-9 * max(1.0, np.max(np.abs(want)))
+        assert np.array_equal(got, want)
+
+
+def test_noalloc_at_its_size_limit_and_with_strided_rhs(cuda, bbk):
+    # n * nrhs exactly at the limit puts the block flags and the status word
+    # at the end of the array; a leading dimension above n checks that only
+    # the first n entries of each right-hand side are read and written.
+    import torch
+    n, blk = 4096, 128
+    nrhs = bbk.SOLVE_NOALLOC_MAX_ELEMENTS // n
+    assert n * nrhs == bbk.SOLVE_NOALLOC_MAX_ELEMENTS
+    f = torch.from_numpy(uniform_symmetric(n, 4097)).to(cuda)
+    perm, pt, _ = bbk.factor_device(f, blk)
+    rng = np.random.default_rng(11)
+    b = torch.from_numpy(rng.standard_normal((nrhs, n))).to(cuda)
+    assert np.array_equal(_solve_noalloc(bbk, f, perm, pt, b).cpu().numpy(),
+                          _solve_existing(bbk, f, perm, pt, b).cpu().numpy())
+    ldb = n + 5
+    wide = torch.from_numpy(rng.standard_normal((3, ldb))).to(cuda)
+    got = _solve_noalloc(bbk, f, perm, pt, wide).cpu().numpy()
+    want = _solve_existing(bbk, f, perm, pt, wide).cpu().numpy()
+    assert np.array_equal(got, want)
+    assert np.array_equal(got[:, n:], wide[:, n:].cpu().numpy())  # padding untouched
 
 
 def test_noalloc_rejects_sizes_beyond_its_scratch(cuda, bbk):
