@@ -1,12 +1,21 @@
 #!/usr/bin/env python
 """LDL^T solve benchmark on B200.
 
-Workload (default): plain FP64 blocked Bunch-Kaufman LDL^T factorization plus
-one solve of the saddle-point KKT matrix [[H, B^T], [B, 0]], n = 10000 with
-H 8000 x 8000 = G G^T / 8000 + 1e-2 I (G Gaussian), B 2000 x 8000 Gaussian,
-block size 128, one right-hand side b ~ N(0, 1).  Seeded synthetic inputs.
+Default workload (the metric's largest single-GPU configuration): plain FP64
+blocked Bunch-Kaufman LDL^T factorization plus the solve of 4 right-hand
+sides for a random symmetric indefinite matrix, n = 40000 (12.8 GB FP64 in
+HBM), entries uniform[-1, 1] plus N(0, 0.01) on the diagonal, block size
+256.  Seeded synthetic inputs.
 
 metric: GFLOP/s = (n^3 / 3) / (time of factorization + solve), whole job.
+The same line carries the metric's other two parts:
+  mixed     FP64 vs low-precision trailing updates (FP32, BF16x3, BF16) +
+            FP64 FGMRES refinement, time to backward error <= 1e-12, on the
+            n = 40000 matrix above and on the ill-conditioned spectral matrix
+            (n = 20000, condition ~1e8, 16 right-hand sides);
+  batched   4096 KKT matrices, n ~ U[16, 512], factored and solved in one
+            persistent launch (CUDA graph), FP64 and FP32 + FP64 refinement,
+            matrices/s against looping the single-matrix path.
 
 Arms:
   (default)          this library on the GPU(s); one process per GPU under
@@ -47,42 +56,54 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--n", type=int, default=10000)
-    ap.add_argument("--h", type=int, default=None, help="H block order (default 0.8 n)")
-    ap.add_argument("--block", type=int, default=128)
-    ap.add_argument("--nrhs", type=int, default=1)
+    ap.add_argument("--workload", default="all", choices=["all", "fp64", "mixed", "batched"],
+                    help="all: the FP64 line with the mixed and batched parts attached (default); "
+                         "fp64: the FP64 line alone; mixed / batched: one part alone, on its own line")
+    ap.add_argument("--matrix", default="random", choices=["random", "kkt", "spectral"],
+                    help="the FP64 line's matrix: random indefinite (n=40000, block 256, 4 RHS; default), "
+                         "KKT saddle point (n=10000, block 128, 1 RHS); mixed alone: random or spectral")
+    ap.add_argument("--n", type=int, default=None)
+    ap.add_argument("--h", type=int, default=None, help="KKT: H block order (default 0.8 n)")
+    ap.add_argument("--block", type=int, default=None)
+    ap.add_argument("--nrhs", type=int, default=None)
     ap.add_argument("--mode", default="fp64", choices=["fp64", "fp64_ordered", "fp32"])
     ap.add_argument("--seed", type=int, default=20240)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU baseline sample time")
-    ap.add_argument("--matrix", default="spectral", choices=["spectral", "random"],
-                    help="mixed: the spectral matrix (n=20000, 16 RHS, condition ~1e8) or the random "
-                         "indefinite one (n=40000, block 256, 4 RHS)")
-    ap.add_argument("--workload", default="kkt", choices=["kkt", "mixed", "batched"],
-                    help="kkt: the headline FP64 factor+solve line; mixed: FP64 vs low-precision "
-                         "updates + FP64 refinement on an ill-conditioned matrix (n=20000, 16 RHS); "
-                         "batched: 4096 KKT matrices, n ~ U[16, 512], one persistent launch")
     ap.add_argument("--count", type=int, default=4096, help="batched: matrices per GPU")
     ap.add_argument("--loop-sample", type=int, default=256,
                     help="batched: matrices timed through the looped single-matrix path")
-    return ap.parse_args()
+    args = ap.parse_args()
+    defaults = {"random": (40000, 256, 4), "kkt": (10000, 128, 1), "spectral": (20000, 128, 16)}
+    dn, db, dr = defaults[args.matrix]
+    args.n = args.n if args.n is not None else dn
+    args.block = args.block if args.block is not None else db
+    args.nrhs = args.nrhs if args.nrhs is not None else dr
+    return args
 
 
 def flops_ldlt(n: int) -> float:
     return n ** 3 / 3.0
 
 
+def matrix_description(kind: str, n: int, h=None) -> str:
+    if kind == "kkt":
+        h = h if h is not None else int(round(0.8 * n))
+        return f"KKT saddle point n={n} (H {h} SPD = G G^T/{h} + 1e-2 I, B Gaussian, zero (2,2) block)"
+    if kind == "spectral":
+        return f"A = Q diag(lam) Q^T, n={n}, |lam| log-uniform [1e-4, 1e4], half negative (condition ~1e8)"
+    return f"random symmetric indefinite n={n} (uniform[-1,1] entries plus N(0, 0.01) on the diagonal)"
+
+
 def workload_config(args, n_used=None) -> dict:
     n = args.n if n_used is None else n_used
-    h = args.h if args.h is not None else int(round(0.8 * args.n))
     return {
-        "workload": f"plain FP64 blocked Bunch-Kaufman LDL^T factor + solve, KKT n={n} "
-                    f"(H {h if n_used is None else int(round(0.8 * n))} SPD, B Gaussian, zero (2,2) block), "
+        "workload": f"plain FP64 blocked Bunch-Kaufman LDL^T factor + solve, "
+                    f"{matrix_description(args.matrix, n, args.h if n_used is None else None)}, "
                     f"block {args.block}, {args.nrhs} RHS",
         "n": n, "block_size": args.block, "nrhs": args.nrhs, "update": args.mode,
-        "l2": "inputs larger than L2 (the n x n FP64 matrix); the input is restored by a device "
-              "copy inside each timed step",
     }
 
 
@@ -192,6 +213,32 @@ def kkt_host(n: int, h: int, seed: int):
     return a
 
 
+def random_indefinite_host(n: int, seed: int):
+    """The random indefinite structure on the host (numpy PCG64): entries
+    uniform[-1, 1], upper triangle mirrored, plus N(0, 0.01) on the diagonal."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    u = rng.uniform(-1.0, 1.0, size=(n, n))
+    a = np.triu(u)
+    a = a + np.triu(a, 1).T
+    a[np.diag_indices(n)] += 0.1 * rng.standard_normal(n)
+    return a
+
+
+def host_matrix(kind: str, n: int, seed: int):
+    """A host matrix of the FP64 line's structure for the CPU reference."""
+    if kind == "kkt":
+        return kkt_host(n, int(round(0.8 * n)), seed)
+    if kind == "spectral":
+        import numpy as np
+        rng = np.random.default_rng(seed)
+        q, _ = np.linalg.qr(rng.standard_normal((n, n)))
+        lam = np.exp(rng.uniform(np.log(1e-4), np.log(1e4), n)) * np.where(rng.permutation(n) < n // 2, -1.0, 1.0)
+        a = (q * lam) @ q.T
+        return (a + a.T) / 2
+    return random_indefinite_host(n, seed)
+
+
 def measure_dgemm_tflops(device) -> float:
     import torch
     n = 8192
@@ -248,7 +295,36 @@ def panel_bytes(n: int, panel_end) -> float:
 # ---------------------------------------------------------------------------
 # this library
 # ---------------------------------------------------------------------------
-def run_b200(args):
+def make_matrix(kind: str, n: int, nrhs: int, seed: int, device, h=None):
+    """The FP64 line's input on the device: (matrix n x n, right-hand sides
+    nrhs x n)."""
+    if kind == "kkt":
+        a, b0 = kkt_device(n, h if h is not None else int(round(0.8 * n)), seed, device)
+        rhs = b0.reshape(1, n).repeat(nrhs, 1).contiguous()
+        return a, rhs
+    if kind == "spectral":
+        a, rhs = spectral_device(n, seed, device)
+        return a, rhs[:nrhs].contiguous()
+    return random_indefinite_device(n, seed, device, nrhs)
+
+
+def traffic_per_unit(key: str, kernel: str):
+    """DRAM bytes per algorithmic unit of `kernel` measured by ncu on the
+    workload `key` (profiles/traffic.json), or None."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["workloads"][key][kernel]["bytes_per_unit"])
+    except (OSError, ValueError, KeyError, TypeError):
+        return None
+
+
+def run_main(args):
+    """The FP64 factor + solve line (every rank a replica), then, on rank 0
+    after the ranks have finished together, the mixed-precision and batched
+    parts of the metric (workload "all")."""
+    import ctypes
+
     import numpy as np
     import torch
     import torch.distributed as dist
@@ -271,9 +347,7 @@ def run_b200(args):
         return reduce_max_over_ranks(x, world, dev)
 
     n, blk, nrhs = args.n, args.block, args.nrhs
-    h = args.h if args.h is not None else int(round(0.8 * n))
-    a0, b0 = kkt_device(n, h, args.seed, dev)
-    rhs0 = b0.repeat(nrhs, 1).contiguous() if nrhs > 1 else b0.reshape(1, n).contiguous()
+    a0, rhs0 = make_matrix(args.matrix, n, nrhs, args.seed, dev, args.h)
     dgemm = measure_dgemm_tflops(dev)
     hbm, hbm_src = measured_hbm_gbs()
 
@@ -283,7 +357,6 @@ def run_b200(args):
     ws_s = torch.empty(bbk.solve_workspace_size(n, nrhs), dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream()
     L = bbk.lib()
-    import ctypes
     nb = (n + blk - 1) // blk
     perm = torch.empty(n, dtype=torch.int32, device=dev)
     pt = torch.empty(n, dtype=torch.int32, device=dev)
@@ -328,10 +401,11 @@ def run_b200(args):
     ms_step = ms / args.steps
     value = world * flops_ldlt(n) / (ms_step / 1e3) / 1e9
 
-    # accuracy of the last step: backward error of the solve (FP64, on device)
-    asym = a0
-    r = rhs0.T - asym @ x.T
-    berr = float((r.abs().amax() / (asym.abs().sum(1).amax() * x.abs().amax() + rhs0.abs().amax())).item())
+    # accuracy of the last step: backward error of every solve (FP64, on device)
+    r = rhs0.T - a0 @ x.T
+    anorm = a0.abs().sum(1).amax()
+    berr = float((r.abs().amax(0) / (anorm * x.T.abs().amax(0) + rhs0.T.abs().amax(0))).max().item())
+    del r
     pe_h = pe.cpu().numpy().tolist()
     pt_h = pt.cpu().numpy()
     n1, n2 = int((pt_h == 1).sum()), int((pt_h == 2).sum())
@@ -350,7 +424,8 @@ def run_b200(args):
     if prof["panel"]["ms"] > 0:
         kernels["panel"] = {
             "bound": "hbm", "achieved": pan_bytes / (prof["panel"]["ms"] / 1e3) / 1e9, "unit": "GB/s",
-            "peak": hbm, "peak_source": hbm_src, "ms": prof["panel"]["ms"], "launches": prof["panel"]["launches"]}
+            "peak": hbm, "peak_source": hbm_src, "ms": prof["panel"]["ms"], "launches": prof["panel"]["launches"],
+            "us_per_pivot_step": prof["panel"]["ms"] * 1e3 / (args.steps * n)}
         kernels["panel"]["frac"] = kernels["panel"]["achieved"] / hbm
     for k in ("finalize", "solve", "init"):
         kernels[k] = {"ms": prof[k]["ms"], "launches": prof[k]["launches"]}
@@ -359,35 +434,32 @@ def run_b200(args):
         v["share"] = (v["ms"] / total_prof) if total_prof > 0 else None
     dom = max(("trailing_update", "panel"), key=lambda k: kernels.get(k, {}).get("ms", 0.0))
     dk = kernels[dom]
-    # DRAM bytes per launch: the measured bytes per unit (profiles/traffic.json,
-    # from an ncu capture of this workload) times the units of an average
+    # DRAM bytes per launch: the bytes per unit an ncu capture of this
+    # workload measured (profiles/traffic.json) times the units of an average
     # launch of this run
     traffic = None
-    traffic_path = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(traffic_path) and dk.get("launches"):
-        try:
-            with open(traffic_path) as fh:
-                per_unit = float(json.load(fh)[dom]["bytes_per_unit"])
-            if dom == "panel":
-                units, k0 = 0.0, 0
-                for e in pe_h:
-                    units += float(e - k0) * (n - k0)
-                    k0 = e
-                units *= args.steps
-            else:
-                units = upd_flops
-            traffic = per_unit * units / dk["launches"]
-        except (OSError, ValueError, KeyError):
-            traffic = None
+    per_unit = traffic_per_unit(f"{args.matrix}_n{n}_b{blk}", dom)
+    if per_unit is not None and dk.get("launches"):
+        if dom == "panel":
+            units, k0 = 0.0, 0
+            for e in pe_h:
+                units += float(e - k0) * (n - k0)
+                k0 = e
+            units *= args.steps
+        else:
+            units = upd_flops
+        traffic = per_unit * units / dk["launches"]
     roofline = {"kernel": dom, "bound": dk["bound"], "achieved": dk["achieved"], "peak": dk["peak"],
-                "unit": dk["unit"], "frac": dk["frac"], "traffic": traffic, "peak_source": dk["peak_source"]}
-    if dom == "panel":
+                "unit": dk["unit"], "frac": dk["frac"], "traffic": traffic, "peak_source": dk["peak_source"],
+                "algorithmic_units": ("2 * width * m(m+1)/2 flops per panel update (m trailing rows), "
+                                      "summed over the launches" if dom == "trailing_update" else
+                                      "24 bytes per panel-strip entry (width x trailing order)")}
+    if "panel" in kernels:
         # The panel is a chain of pivot steps, each needing one grid-wide
         # exchange (argmax + published scalars) before the next can start:
         # its floor is one bare exchange per step, measured here on the same
         # grid (bbk_probe_exchange_ns: back-to-back exchanges, each with a
         # release fence).
-        import torch
         sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
         grid = max(min(sms, -(-n // 64)), -(-n // 576))  # the panel launch's grid (64 columns per CTA)
         try:
@@ -396,13 +468,16 @@ def run_b200(args):
             x_ns = None
         per_step_us = kernels["panel"]["ms"] * 1e3 / (args.steps * n)
         if x_ns:
-            roofline["latency"] = {"unit": "us per pivot step", "achieved": per_step_us,
-                                   "floor": x_ns / 1e3, "frac": (x_ns / 1e3) / per_step_us,
-                                   "floor_source": "one bare grid exchange per pivot step, measured live",
-                                   "grid": int(grid)}
+            kernels["panel"]["latency"] = {"unit": "us per pivot step", "achieved": per_step_us,
+                                           "floor": x_ns / 1e3, "frac": (x_ns / 1e3) / per_step_us,
+                                           "floor_source": "one bare grid exchange per pivot step, "
+                                                           "measured live", "grid": int(grid)}
+            if dom == "panel":
+                roofline["latency"] = kernels["panel"]["latency"]
 
     # end to end through the host-buffer C ABI (pinned host memory)
     e2e = None
+    del work
     if not args.no_e2e:
         ha = a0.cpu().pin_memory()
         hb = rhs0.cpu().pin_memory()
@@ -423,7 +498,7 @@ def run_b200(args):
 
         restore()
         e2e_call()
-        k_e2e = max(1, min(args.steps, 5))
+        k_e2e = max(1, min(args.steps, args.e2e_steps))
         tot_ms = 0.0
         for _ in range(k_e2e):
             restore()  # the caller's input is restored outside the timed call
@@ -445,29 +520,51 @@ def run_b200(args):
         e2e = {"value": world * flops_ldlt(n) / (ems / 1e3) / 1e9, "unit": UNIT, "ms_per_step": ems,
                "steps": k_e2e, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "api": "bbk_factor_solve_host (host buffers, pinned): H2D of the matrix's upper triangle "
-                      "(64-row wedges) and rhs, factor, solve, D2H of compact factors, pivots and "
-                      "solution, inside each timed step"}
-
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_sample(args, target_s=args.cpu_seconds)
+                      "(64-row wedges) and right-hand sides, factor, solve, D2H of compact factors, pivots "
+                      "and solutions, inside each timed step"}
+        del ha, hb, hwork, hx
 
     if world > 1:
         dist.destroy_process_group()
     if rank != 0:
         return
+
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample(args, target_s=args.cpu_seconds)
+
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.mode != "fp32" else "f64+f32-update",
-        "data": "synthetic: seeded KKT saddle-point matrix (torch Gaussian generators on the device)",
+        "data": f"synthetic: seeded {matrix_description(args.matrix, n, args.h)} (torch generators on the device)",
         "config": dict(workload_config(args), parallelism=f"replicas x{world} (one matrix per GPU)",
-                       seed=args.seed),
+                       seed=args.seed,
+                       l2=f"inputs larger than L2 (the n x n FP64 matrix, {8 * n * n / 1e9:.1f} GB); the input "
+                          "is restored by a device copy inside each timed step"),
         "e2e": e2e, "roofline": roofline, "kernels": kernels, "cpu_baseline": cpu,
         "clocks": clocks, "gpu_launches": launches,
-        "accuracy": {"backward_error": berr, "pivots_1x1": n1, "pivots_2x2": n2, "boundary_shifts": shifts},
+        "accuracy": {"backward_error_max_over_rhs": berr, "pivots_1x1": n1, "pivots_2x2": n2,
+                     "boundary_shifts": shifts},
         "fp64_dgemm_tflops": dgemm,
     }
+    if args.workload == "all":
+        # the metric's other parts, on this GPU, after the timed line
+        fp64_ref = {"ms": ms_step, "backward_error": berr, "refine_steps": 0,
+                    "how": "the FP64 line's factor + solve time per step (input restore included)"}
+        modes = ("fp32", "bf16x3", "bf16") if args.matrix == "random" else ("fp32", "bf16x3")
+        mixed = {f"{args.matrix}_n{n}": mixed_arms(a0, rhs0, blk, modes, fp64=fp64_ref, x64=x,
+                                                   what=f"{matrix_description(args.matrix, n, args.h)}, "
+                                                        f"block {blk}, {nrhs} RHS")}
+        del a0, rhs0, x
+        torch.cuda.empty_cache()
+        a3, rhs3 = spectral_device(20000, args.seed, dev)
+        mixed["spectral_n20000"] = mixed_arms(a3, rhs3, 128, ("fp32", "bf16x3"),
+                                              what=f"{matrix_description('spectral', 20000)}, block 128, 16 RHS")
+        del a3, rhs3
+        torch.cuda.empty_cache()
+        line["mixed"] = mixed
+        line["batched"] = batched_results(args, 1, 0, dev)
     print(json.dumps(line), flush=True)
 
 
@@ -494,7 +591,7 @@ def _cpu_factor(lib, kind, a, blk):
 
 def _pick_sample_n(lib, kind, args, target_s: float) -> int:
     n_cal = 1536
-    a = kkt_host(n_cal, int(round(0.8 * n_cal)), args.seed)
+    a = host_matrix(args.matrix, n_cal, args.seed)
     t = _cpu_factor(lib, kind, a, args.block)
     rate = flops_ldlt(n_cal) / max(t, 1e-6)
     n_s = int((3.0 * rate * target_s) ** (1.0 / 3.0))
@@ -506,12 +603,12 @@ def cpu_baseline_sample(args, target_s: float) -> dict:
     lib, kind = _reference_lib()
     cores = lib.threads() if kind == "reference" else 1
     n_s = _pick_sample_n(lib, kind, args, target_s)
-    a = kkt_host(n_s, int(round(0.8 * n_s)), args.seed)
+    a = host_matrix(args.matrix, n_s, args.seed)
     t = _cpu_factor(lib, kind, a, args.block)
     return {"value": flops_ldlt(n_s) / t / 1e9, "unit": UNIT, "cores": cores, "kind": kind,
-            "sample": f"one factorization of a KKT matrix of the same structure at n={n_s} "
-                      f"(H {int(round(0.8 * n_s))}), block {args.block}, ctor + Factorize() timed; "
-                      "the reference has no solve (O(n^2), not timed)",
+            "sample": f"one factorization of a {matrix_description(args.matrix, n_s)}, block {args.block}, "
+                      f"ctor + Factorize() timed with {cores} threads (a bounded sample: the reference at "
+                      f"n={args.n} would take far longer than a benchmark run); the reference has no solve",
             "seconds": t}
 
 
@@ -525,21 +622,24 @@ def run_reference(args):
     total_steps = max(1, args.steps) + max(0, args.warmup)
     per_step = max(2.0, min(30.0, 150.0 / total_steps))
     n_s = _pick_sample_n(lib, kind, args, per_step)
-    a = kkt_host(n_s, int(round(0.8 * n_s)), args.seed)
+    a = host_matrix(args.matrix, n_s, args.seed)
     for _ in range(max(0, args.warmup)):
         _cpu_factor(lib, kind, a, args.block)
     times = [_cpu_factor(lib, kind, a, args.block) for _ in range(max(1, args.steps))]
     tot = sum(times)
     value = flops_ldlt(n_s) * len(times) / tot / 1e9
-    sample = (f"each step one factorization of a KKT matrix of the same structure at n={n_s} "
-              f"(H {int(round(0.8 * n_s))}), block {args.block}, ctor + Factorize() timed with "
-              f"{cores} OpenMP threads; the reference has no solve")
+    sample = (f"each step one factorization of a {matrix_description(args.matrix, n_s)}, block "
+              f"{args.block}, ctor + Factorize() timed with {cores} OpenMP threads; n is bounded so the run "
+              f"ends in minutes (the reference at n={args.n} would take over an hour); the reference has no "
+              "solve")
+    cfg = workload_config(args, n_used=n_s)
+    cfg["l2"] = "host memory (CPU run): every step factors the same host matrix, copied by the reference's constructor"
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": len(times),
         "warmup": args.warmup, "ms_per_step": tot / len(times) * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "impl": "reference",
-        "data": "synthetic: seeded KKT saddle-point matrix (numpy PCG64)",
-        "config": workload_config(args, n_used=n_s),
+        "data": f"synthetic: seeded {matrix_description(args.matrix, n_s)} (numpy PCG64)",
+        "config": cfg,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -579,28 +679,22 @@ def spectral_device(n: int, seed: int, device, lo=1e-4, hi=1e4):
     return a, rhs
 
 
-def run_mixed(args):
-    """FP64 path vs low-precision trailing updates + FP64 GMRES-IR: time to a
-    solution with backward error <= 1e-12 (every one of 16 right-hand sides),
-    and the forward error against the FP64 path's solution."""
+def mixed_arms(a0, rhs, blk: int, modes, fp64=None, x64=None, what: str = "", tol: float = 1e-12) -> dict:
+    """Time to a solution with backward error <= tol for every right-hand
+    side (rows of `rhs`): the FP64 path (factor + solve; `fp64` / `x64` when
+    the caller already timed it) against each low-precision trailing update
+    in `modes` followed by FP64 FGMRES refinement (restart 50, at most 3
+    outer steps) against the original matrix.  Each arm: one untimed run,
+    then one timed run (CUDA events and the host clock, the larger)."""
     import torch
 
     import blockedbunchkaufmanldlt_b200 as bbk
-    dev = torch.device("cuda", 0)
-    torch.cuda.set_device(0)
-    rand = args.matrix == "random"
-    n = args.n if args.n != 10000 else (40000 if rand else 20000)
-    blk = args.block if (args.block != 128 or not rand) else 256
-    if rand:
-        a0, rhs = random_indefinite_device(n, args.seed, dev, 4)
-    else:
-        a0, rhs = spectral_device(n, args.seed, dev)
-    nrhs = rhs.shape[0]
-    tol = 1e-12
+    n = a0.shape[0]
+    anorm = a0.abs().sum(1).amax()
 
     def berr(x):
         r = rhs.T - a0 @ x.T
-        return float((r.abs().amax(0) / (a0.abs().sum(1).amax() * x.T.abs().amax(0) + rhs.T.abs().amax(0))).max())
+        return float((r.abs().amax(0) / (anorm * x.T.abs().amax(0) + rhs.T.abs().amax(0))).max())
 
     def timed(fn):
         torch.cuda.synchronize()
@@ -613,20 +707,22 @@ def run_mixed(args):
         return out, max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3)
 
     results = {}
-    # FP64: factor + solve (+ FP64 refinement only if the plain solve misses tol)
-    for _ in range(1 + max(0, min(args.warmup, 1))):
-        w = a0.clone()
+    if fp64 is None:
+        for _ in range(2):
+            w = a0.clone()
 
-        def fp64_path():
-            perm, pt, _ = bbk.factor_device(w, blk, mode="fp64")
-            x = rhs.clone()
-            bbk.solve_device(w, perm, pt, x)
-            return x, perm, pt
-        (x64, perm64, pt64), ms = timed(fp64_path)
-    e64 = berr(x64)
-    results["fp64"] = {"ms": ms, "backward_error": e64, "refine_steps": 0}
-    for mode in (("fp32", "bf16x3", "bf16") if rand else ("fp32", "bf16x3")):
-        for _ in range(1 + max(0, min(args.warmup, 1))):
+            def fp64_path():
+                perm, pt, _ = bbk.factor_device(w, blk, mode="fp64")
+                x = rhs.clone()
+                bbk.solve_device(w, perm, pt, x)
+                return x
+            x64, ms = timed(fp64_path)
+            del w
+        fp64 = {"ms": ms, "backward_error": berr(x64), "refine_steps": 0}
+    results["fp64"] = fp64
+    xnorm = x64.abs().amax()
+    for mode in modes:
+        for _ in range(2):
             w = a0.clone()
 
             def mixed_path():
@@ -635,21 +731,44 @@ def run_mixed(args):
                                                    method="gmres", restart=50)
                 return x, info
             (x, info), ms = timed(mixed_path)
-        fe = float((x - x64).abs().amax() / x64.abs().amax())
-        results[mode] = {"ms": ms, "backward_error": berr(x), "initial_backward_error": info.initial_backward_error,
-                         "refine_steps": info.iterations,
-                         "gmres_steps": info.inner_iterations, "converged": bool(info.converged),
-                         "forward_error_vs_fp64": fe, "speedup_vs_fp64": results["fp64"]["ms"] / ms}
+            del w
+        fe = float((x - x64).abs().amax() / xnorm)
+        results[mode + "+ir"] = {
+            "ms": ms, "backward_error": berr(x), "initial_backward_error": info.initial_backward_error,
+            "refine_steps": info.iterations, "gmres_steps": info.inner_iterations,
+            "converged": bool(info.converged), "forward_error_vs_fp64": fe,
+            "speedup_vs_fp64": fp64["ms"] / ms}
+        del x
+    conv = [k for k, v in results.items() if k != "fp64" and v["converged"]]
+    best = min(conv, key=lambda k: results[k]["ms"]) if conv else None
+    return {"workload": what, "n": n, "block_size": blk, "nrhs": int(rhs.shape[0]), "tol": tol,
+            "arms": results, "fastest_converged_low_precision": best,
+            "best_speedup_vs_fp64": results[best]["speedup_vs_fp64"] if best else None,
+            "fp64_meets_tol": results["fp64"]["backward_error"] <= tol}
+
+
+def run_mixed(args):
+    """The mixed-precision part alone on its own line: --matrix random (the
+    n=40000 random indefinite matrix, block 256, 4 RHS) or spectral (n=20000,
+    condition ~1e8, 16 RHS)."""
+    import torch
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(0)
+    rand = args.matrix != "spectral"
+    n = args.n if args.matrix != "kkt" else 40000
+    if rand:
+        a0, rhs = random_indefinite_device(n, args.seed, dev, args.nrhs)
+        modes = ("fp32", "bf16x3", "bf16")
+    else:
+        a0, rhs = spectral_device(n, args.seed, dev)
+        modes = ("fp32", "bf16x3")
+    res = mixed_arms(a0, rhs, args.block, modes,
+                     what=f"{matrix_description('random' if rand else 'spectral', n)}, block {args.block}, "
+                          f"{rhs.shape[0]} RHS")
     line = {"metric": "time to backward error <= 1e-12, FP64 vs low-precision update + FP64 GMRES-IR",
             "unit": "ms", "higher_is_better": False, "n_gpus": 1, "dtype": "f64 (panel, residual) + update",
-            "data": ("synthetic: seeded uniform[-1,1] symmetric plus N(0, 0.01) on the diagonal; "
-                     f"{nrhs} RHS N(0,1)") if rand else
-                    ("synthetic: A = Q diag(lam) Q^T, Q from QR of a seeded Gaussian, |lam| log-uniform "
-                     "[1e-4, 1e4], half negative; 16 RHS N(0,1)"),
-            "config": {"workload": (f"large FP64 vs mixed, random indefinite n={n}, block {blk}, {nrhs} RHS"
-                                    if rand else f"mixed precision, n={n}, block {blk}, 16 RHS, condition ~1e8"),
-                       "n": n, "block_size": blk, "nrhs": nrhs},
-            "results": results}
+            "data": "synthetic: seeded, generated on the device", "config": {"workload": res["workload"]},
+            "results": res}
     print(json.dumps(line), flush=True)
 
 
@@ -665,13 +784,9 @@ def run_batched(args):
     block), n ~ U[16, 512], one right-hand side each; FP64 and FP32 + FP64
     refinement; one persistent launch replayed from a CUDA graph.  Compared
     with looping the single-matrix path over a subset."""
-    import ctypes
-
     import torch
     import torch.distributed as dist
 
-    import blockedbunchkaufmanldlt_b200 as bbk
-    from blockedbunchkaufmanldlt_b200 import tuning
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -679,6 +794,22 @@ def run_batched(args):
     dev = torch.device("cuda", local)
     if world > 1:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    line = batched_results(args, world, rank, dev)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def batched_results(args, world: int, rank: int, dev) -> dict:
+    """The batched part (every rank its own batch; collectives only for the
+    max over ranks when world > 1): the line's fields as a dict."""
+    import ctypes
+
+    import torch
+
+    import blockedbunchkaufmanldlt_b200 as bbk
+    from blockedbunchkaufmanldlt_b200 import tuning
 
     def max_over_ranks(v: float) -> float:
         return reduce_max_over_ranks(v, world, dev)
@@ -849,10 +980,7 @@ def run_batched(args):
                                                      "FP64 FMA and DMMA peaks are equal on B200)"},
         "clocks": clocks, "gpu_launches": 1,
     }
-    if rank == 0:
-        print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.destroy_process_group()
+    return line
 
 
 def run_reference_batched(args):
@@ -918,7 +1046,7 @@ def main():
     elif args.workload == "mixed":
         run_mixed(args)
     else:
-        run_b200(args)
+        run_main(args)
 
 
 if __name__ == "__main__":
