@@ -46,9 +46,9 @@ REFINE_GMRES = 1
 EXPORTS = (
     "bbk_abi_version", "bbk_last_error", "bbk_status_string", "bbk_kernel_launch_count",
     "bbk_set_wait_timeout_ns", "bbk_probe_bounded_wait", "bbk_probe_exchange_ns", "bbk_factor_workspace_size",
-    "bbk_factor_device", "bbk_factor_device_async", "bbk_factor_device_logged", "bbk_factor_host",
+    "bbk_factor_device", "bbk_factor_device_async", "bbk_factor_device_ex", "bbk_factor_host",
     "bbk_solve_workspace_size", "bbk_solve_device", "bbk_solve_host", "bbk_factor_solve_host",
-    "bbk_reconstruct_device", "bbk_scale_one_by_one", "bbk_scale_two_by_two",
+    "bbk_reconstruct_device", "bbk_extract_ld_device", "bbk_sampled_residual_device", "bbk_scale_one_by_one", "bbk_scale_two_by_two",
     "bbk_update_trailing_block", "bbk_profile_begin", "bbk_profile_end", "bbk_panel_stats", "bbk_panel_stats_raw", "bbk_solve_device_noalloc",
     "bbk_solve_refined_workspace_size", "bbk_solve_refined_device",
     "bbk_batched_workspace_size", "bbk_batched_plan", "bbk_batched_factor_solve",
@@ -134,8 +134,8 @@ def lib() -> ctypes.CDLL:
         "bbk_factor_device": ([_c_int, _c_int, _vp, _c_ll, _vp, _vp, _vp, _c_int, _vp, _c_sz, _vp], _c_int),
         "bbk_factor_device_async": ([_c_int, _c_int, _vp, _c_ll, _vp, _vp, _vp, _c_int, _vp, _c_sz,
                                      _vp, _vp], _c_int),
-        "bbk_factor_device_logged": ([_c_int, _c_int, _vp, _c_ll, _vp, _vp, _vp, _c_int, _vp, _vp, _c_sz,
-                                      _vp, _vp], _c_int),
+        "bbk_factor_device_ex": ([_c_int, _c_int, _vp, _c_ll, _vp, _vp, _vp, _c_int, _vp, _vp, _c_sz,
+                                  _vp, _vp], _c_int),
         "bbk_factor_host": ([_c_int, _c_int, _vp, _c_ll, _vp, _vp, _vp, _c_int], _c_int),
         "bbk_solve_workspace_size": ([_c_int, _c_int], _c_sz),
         "bbk_solve_device": ([_c_int, _vp, _c_ll, _vp, _vp, _c_int, _vp, _c_ll, _vp, _c_sz, _vp], _c_int),
@@ -152,6 +152,9 @@ def lib() -> ctypes.CDLL:
         "bbk_factor_solve_host": ([_c_int, _c_int, _vp, _c_ll, _vp, _vp, _vp, _c_int, _vp, _c_ll,
                                    _c_int], _c_int),
         "bbk_reconstruct_device": ([_c_int, _vp, _c_ll, _vp, _vp, _vp, _c_ll, _vp], _c_int),
+        "bbk_extract_ld_device": ([_c_int, _vp, _c_ll, _vp, _vp, _c_ll, _vp, _c_ll, _vp], _c_int),
+        "bbk_sampled_residual_device": ([_c_int, _vp, _c_ll, _vp, _c_ll, _vp, _vp, _c_int, _vp, _vp, _vp, _vp],
+                                        _c_int),
         "bbk_scale_one_by_one": ([_c_int, _c_dbl, _vp, _c_int, _vp, _c_int, _vp], _c_int),
         "bbk_scale_two_by_two": ([_c_int, _c_dbl, _c_dbl, _c_dbl, _vp, _c_int, _vp, _c_int, _vp,
                                   _c_int, _vp, _c_int, _vp], _c_int),
@@ -265,11 +268,19 @@ PIVOT_LOG_WORDS = 4  # |W(p,p)|, omega, sigma, |W(r,r)| per factored position
 ALPHA = 0.6403882032022076  # the Bunch-Kaufman threshold (1 + sqrt 17) / 8
 
 
-def factor_device_logged(a, block_size: int, mode="fp64", stream=None):
-    """factor_device plus the decision log of bbk_factor_device_logged:
+class FactorExtras(ctypes.Structure):
+    """bbk_factor_extras"""
+    _fields_ = [("pivot_log", ctypes.c_void_p), ("workspace_rows", ctypes.c_void_p),
+                ("workspace_ld", ctypes.c_longlong)]
+
+
+def factor_device_logged(a, block_size: int, mode="fp64", stream=None, workspace_rows=None):
+    """factor_device plus the optional outputs of bbk_factor_device_ex:
     returns (perm, pivot_types, panel_end, log) with log an n x 4 float64
     device tensor (|W(p,p)|, omega, sigma, |W(r,r)| at each position where a
-    pivot step started; NaN elsewhere and where no candidate was needed)."""
+    pivot step started; NaN elsewhere and where no candidate was needed).
+    ``workspace_rows`` (CUDA float64, n x ld, optional) receives each panel's
+    W rows at its trailing columns."""
     import torch
     if a.dtype != torch.float64 or not a.is_cuda or a.dim() != 2 or a.stride(1) != 1:
         raise InvalidArgument(BBK_ERR_INVALID_ARGUMENT, "need a row-major CUDA float64 matrix")
@@ -280,11 +291,12 @@ def factor_device_logged(a, block_size: int, mode="fp64", stream=None):
     pe = torch.empty(max(nb, 1), dtype=torch.int32, device=a.device)
     log = torch.empty(n, PIVOT_LOG_WORDS, dtype=torch.float64, device=a.device)
     status = torch.zeros(1, dtype=torch.int32, device=a.device)
-    check(lib().bbk_factor_device_logged(n, block_size, ctypes.c_void_p(a.data_ptr()), a.stride(0),
-                                         ctypes.c_void_p(perm.data_ptr()), ctypes.c_void_p(pt.data_ptr()),
-                                         ctypes.c_void_p(pe.data_ptr()), _mode(mode),
-                                         ctypes.c_void_p(log.data_ptr()), None, 0,
-                                         ctypes.c_void_p(status.data_ptr()), _stream_ptr(stream)))
+    ex = FactorExtras(log.data_ptr(), workspace_rows.data_ptr() if workspace_rows is not None else None,
+                      workspace_rows.stride(0) if workspace_rows is not None else 0)
+    check(lib().bbk_factor_device_ex(n, block_size, ctypes.c_void_p(a.data_ptr()), a.stride(0),
+                                     ctypes.c_void_p(perm.data_ptr()), ctypes.c_void_p(pt.data_ptr()),
+                                     ctypes.c_void_p(pe.data_ptr()), _mode(mode), ctypes.byref(ex), None, 0,
+                                     ctypes.c_void_p(status.data_ptr()), _stream_ptr(stream)))
     torch.cuda.current_stream().synchronize() if stream is None else stream.synchronize()
     st = int(status.item())
     if st != BBK_OK:
@@ -360,6 +372,34 @@ def solve_refined_device(a, f, perm, pivot_types, b, tol=1e-12, max_iter=30, met
                                          ctypes.c_void_p(x.data_ptr()), x.stride(0), tol, max_iter, meth,
                                          restart, ctypes.byref(info), ws_ptr, ws_bytes, _stream_ptr(stream)))
     return (x if b.dim() == 2 else x.reshape(n)), info
+
+
+def sampled_residual_device(a, f, perm, pivot_types, rows, cols, stream=None) -> float:
+    """The reference stress test's sampled relative residual of the compact
+    factors ``f`` against the original ``a`` (CUDA float64, upper triangles),
+    at the sampled entries (rows[k], cols[k]) (CUDA int32 tensors)."""
+    n = f.shape[0]
+    out = ctypes.c_double(0.0)
+    check(lib().bbk_sampled_residual_device(n, ctypes.c_void_p(a.data_ptr()), a.stride(0),
+                                            ctypes.c_void_p(f.data_ptr()), f.stride(0),
+                                            ctypes.c_void_p(perm.data_ptr()),
+                                            ctypes.c_void_p(pivot_types.data_ptr()), rows.numel(),
+                                            ctypes.c_void_p(rows.data_ptr()), ctypes.c_void_p(cols.data_ptr()),
+                                            ctypes.byref(out), _stream_ptr(stream)))
+    return out.value
+
+
+def extract_ld_device(f, pivot_types, stream=None):
+    """Dense (L, D) of the compact factors ``f`` (CUDA float64, n x ldf) on
+    the device: the reference's LFactor() / DFactor()."""
+    import torch
+    n = f.shape[0]
+    l = torch.empty(n, n, dtype=torch.float64, device=f.device)
+    d = torch.empty(n, n, dtype=torch.float64, device=f.device)
+    check(lib().bbk_extract_ld_device(n, ctypes.c_void_p(f.data_ptr()), f.stride(0),
+                                      ctypes.c_void_p(pivot_types.data_ptr()), ctypes.c_void_p(l.data_ptr()), n,
+                                      ctypes.c_void_p(d.data_ptr()), n, _stream_ptr(stream)))
+    return l, d
 
 
 def reconstruct_device(f, perm, pivot_types, stream=None):

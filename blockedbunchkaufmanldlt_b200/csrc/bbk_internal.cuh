@@ -236,6 +236,7 @@ int launch_init(int n, int* perm, int* pivot_types, DeviceState* st,
                 unsigned long long* slots, size_t slot_words, cudaStream_t s);
 int launch_panel(const FactorPlan& plan, int panel, cudaStream_t s);
 int launch_finalize(const FactorPlan& plan, int panel, cudaStream_t s);
+int launch_wrows(const FactorPlan& plan, int panel, cudaStream_t s);
 int launch_update(const FactorPlan& plan, int panel, cudaStream_t s);
 int launch_status_copy(const DeviceState* st, int* status_out, cudaStream_t s);
 int launch_probe_wait(int ctas, int nslots, int iters, unsigned long long timeout_ns,
@@ -266,9 +267,14 @@ int refine_enqueue(int n, const double* a, long long lda, const double* f, long 
                    const int* perm, const int* pt, int nrhs, const double* b, double* x, double tol,
                    int max_iter, int method, int restart, double* work, bbk_refine_info* info,
                    cudaStream_t s);
+size_t reconstruct_work_doubles(int n);
 int reconstruct_enqueue(int n, const double* f, long long ldf, const int* perm,
                         const int* pivot_types, double* out, long long ldo,
                         double* work, cudaStream_t s);
+int extract_ld_enqueue(int n, const double* f, long long ldf, const int* pivot_types, double* l,
+                       long long ldl, double* d, long long ldd, cudaStream_t s);
+int launch_upper_product(int n, const double* m, const double* u, long long ld, double* c,
+                         cudaStream_t s);
 
 // Everything a factorization's kernels need: the caller's matrix and the
 // carved-up workspace.
@@ -306,5 +312,7 @@ struct FactorPlan {
   int kpad = 0;              // BF16 update: panel width rounded up to 32 (k pitch of hsplit)
   size_t hstride = 0;        // BF16 update: elements per operand term (n_pad x kpad)
   double* pivlog = nullptr;  // optional decision log (kPivLogWords doubles per position)
+  double* wrows = nullptr;   // optional copy of each panel's W rows at its trailing columns
+  long long ld_wrows = 0;
 };
 }  // namespace bbk

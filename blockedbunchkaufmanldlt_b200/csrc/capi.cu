@@ -199,6 +199,7 @@ static int enqueue_factor(FactorPlan& plan, int* status_device, cudaStream_t s) 
   for (int panel = 0; panel < plan.nb; ++panel) {
     if ((rc = profiled(kProfPanel, s, [&] { return launch_panel(plan, panel, s); }))) return rc;
     if ((rc = profiled(kProfFinalize, s, [&] { return launch_finalize(plan, panel, s); }))) return rc;
+    if (plan.wrows && (rc = launch_wrows(plan, panel, s))) return rc;
     if ((rc = profiled(kProfUpdate, s, [&] { return launch_update(plan, panel, s); }))) return rc;
   }
   return launch_status_copy(plan.state, status_device, s);
@@ -315,11 +316,14 @@ size_t bbk_factor_workspace_size(int n, int block_size) {
 }
 
 static int factor_async(int n, int block_size, double* a, long long lda, int* perm,
-                        int* pivot_types, int* panel_end, int update_mode, double* pivot_log,
+                        int* pivot_types, int* panel_end, int update_mode, const bbk_factor_extras* extras,
                         void* workspace, size_t workspace_bytes, int* status_device,
                         void* stream) {
   int rc = validate_factor_args(n, block_size, a, lda, perm, pivot_types, update_mode);
   if (rc) return rc;
+  double* pivot_log = extras ? extras->pivot_log : nullptr;
+  if (extras && extras->workspace_rows && extras->workspace_ld < n)
+    return set_error(BBK_ERR_INVALID_ARGUMENT, "workspace_ld (%lld) < n (%d)", extras->workspace_ld, n);
   if ((rc = check_device())) return rc;
   if (n > panel_max_n())
     return set_error(BBK_ERR_INVALID_ARGUMENT, "n = %d exceeds this device's panel limit %d", n,
@@ -339,6 +343,8 @@ static int factor_async(int n, int block_size, double* a, long long lda, int* pe
   plan.timeout_ns = wait_timeout_ns();
   plan.stats = g_panel_stats_on ? g_panel_stats : nullptr;
   plan.pivlog = pivot_log;
+  plan.wrows = extras ? extras->workspace_rows : nullptr;
+  plan.ld_wrows = extras ? extras->workspace_ld : 0;
   if (pivot_log) {
     // all-ones bytes: NaN at every position no decision writes
     BBK_CUDA_TRY(cudaMemsetAsync(pivot_log, 0xff, static_cast<size_t>(n) * kPivLogWords * sizeof(double), s));
@@ -375,12 +381,10 @@ int bbk_factor_device_async(int n, int block_size, double* a, long long lda, int
                       workspace, workspace_bytes, status_device, stream);
 }
 
-int bbk_factor_device_logged(int n, int block_size, double* a, long long lda, int* perm,
-                             int* pivot_types, int* panel_end, int update_mode,
-                             double* pivot_log, void* workspace, size_t workspace_bytes,
-                             int* status_device, void* stream) {
-  if (pivot_log == nullptr) return set_error(BBK_ERR_INVALID_ARGUMENT, "null pivot log");
-  return factor_async(n, block_size, a, lda, perm, pivot_types, panel_end, update_mode, pivot_log,
+int bbk_factor_device_ex(int n, int block_size, double* a, long long lda, int* perm, int* pivot_types,
+                         int* panel_end, int update_mode, const bbk_factor_extras* extras, void* workspace,
+                         size_t workspace_bytes, int* status_device, void* stream) {
+  return factor_async(n, block_size, a, lda, perm, pivot_types, panel_end, update_mode, extras,
                       workspace, workspace_bytes, status_device, stream);
 }
 
@@ -668,10 +672,23 @@ int bbk_reconstruct_device(int n, const double* factors, long long ldf, const in
   if (rc) return rc;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   double* m = nullptr;
-  BBK_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&m),
-                               static_cast<size_t>(n) * n * sizeof(double), s));
+  BBK_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&m), reconstruct_work_doubles(n) * sizeof(double), s));
   rc = reconstruct_enqueue(n, factors, ldf, perm, pivot_types, out, ldo, m, s);
   cudaFreeAsync(m, s);
+  if (rc) return rc;
+  BBK_CUDA_TRY(cudaStreamSynchronize(s));
+  return BBK_OK;
+}
+
+int bbk_extract_ld_device(int n, const double* factors, long long ldf, const int* pivot_types, double* l,
+                          long long ldl, double* d, long long ldd, void* stream) {
+  if (n <= 0) return set_error(BBK_ERR_INVALID_ARGUMENT, "matrix size must be positive");
+  if (!factors || !pivot_types || (!l && !d) || ldf < n || (l && ldl < n) || (d && ldd < n))
+    return set_error(BBK_ERR_INVALID_ARGUMENT, "bad extraction arguments");
+  int rc = check_device();
+  if (rc) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  rc = extract_ld_enqueue(n, factors, ldf, pivot_types, l, ldl, d, ldd, s);
   if (rc) return rc;
   BBK_CUDA_TRY(cudaStreamSynchronize(s));
   return BBK_OK;

@@ -37,6 +37,7 @@
 // row as keeping its pivot would leave it and reduces that row's argmax in
 // the same exchange, so when the pivot is kept (most steps of saddle-point
 // matrices) the next step starts without a row exchange.
+#include <algorithm>
 #include <climits>
 #include <cstdio>
 #include <cstdlib>
@@ -1277,6 +1278,32 @@ int launch_panel(const FactorPlan& plan, int panel, cudaStream_t s) {
   void* kargs[] = {&P};
   cudaError_t err = cudaLaunchCooperativeKernel(fn, dim3(plan.grid), dim3(kBlock), kargs, bytes, s);
   if (err != cudaSuccess) return cuda_error(err, "cudaLaunchCooperativeKernel(panel)");
+  count_launch();
+  return BBK_OK;
+}
+
+namespace {
+// The panel's W rows at the trailing columns (x >= e, final column order,
+// as the panel kernel left them for the update) into the caller's array.
+__global__ void wrows_kernel(const DeviceState* st, int panel, int n, const double* w, long long ldw,
+                             double* out, long long ldo) {
+  if (ld_relaxed_s32(&st->abort)) return;
+  const int k0 = ldcg(&st->kstart[panel & 1]);
+  const int e = ldcg(&st->kstart[(panel + 1) & 1]);
+  const long long width = n - e, total = static_cast<long long>(e - k0) * width;
+  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int q = static_cast<int>(t / width), x = e + static_cast<int>(t % width);
+    out[static_cast<long long>(k0 + q) * ldo + x] = w[q * ldw + x];
+  }
+}
+}  // namespace
+
+int launch_wrows(const FactorPlan& plan, int panel, cudaStream_t s) {
+  const long long work = static_cast<long long>(plan.b + 1) * plan.n;
+  const int grid = static_cast<int>(std::max(1LL, std::min(4096LL, (work + 255) / 256)));
+  wrows_kernel<<<grid, 256, 0, s>>>(plan.state, panel, plan.n, plan.w, plan.ldw, plan.wrows, plan.ld_wrows);
+  BBK_CUDA_TRY(cudaGetLastError());
   count_launch();
   return BBK_OK;
 }

@@ -276,50 +276,72 @@ __global__ void reset_flags_kernel(int* flags, int count) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) flags[i] = 0;
 }
 
-// M = L D (row-major n x n), M(i,k) for k <= i+1.
-__global__ void ld_kernel(int n, const double* f, long long ldf, const int* pt, double* m) {
+// L(row, col) of the compact factors: unit diagonal, F(col, row) below it
+// except the coupling entry of a 2x2 pivot (ExtractRegularFactorsFromCompact,
+// src/block_ldlt_decomposition.cc:746-763).
+__device__ __forceinline__ double l_entry(const double* f, long long ldf, const int* pt, int row, int col) {
+  if (row == col) return 1.0;
+  if (row < col) return 0.0;
+  if (pt[col] == 2 && row == col + 1) return 0.0;
+  return f[static_cast<long long>(col) * ldf + row];
+}
+
+// M = L D and U = L^T (both ld x ld, zero outside the order n): the two
+// operands of the reconstruction product.
+__global__ void ld_lt_kernel(int n, const double* f, long long ldf, const int* pt, long long ld, double* m,
+                             double* u) {
+  const long long total = ld * ld;
+  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int i = static_cast<int>(t / ld), k = static_cast<int>(t % ld);
+    double mv = 0.0, uv = 0.0;
+    if (i < n && k < n) {
+      if (pt[k] == 2 && k + 1 < n) {
+        mv = l_entry(f, ldf, pt, i, k) * f[k * ldf + k] + l_entry(f, ldf, pt, i, k + 1) * f[k * ldf + k + 1];
+      } else if (pt[k] == -2 && k > 0) {
+        mv = l_entry(f, ldf, pt, i, k - 1) * f[(k - 1) * ldf + k] + l_entry(f, ldf, pt, i, k) * f[k * ldf + k];
+      } else {
+        mv = l_entry(f, ldf, pt, i, k) * f[k * ldf + k];
+      }
+      uv = l_entry(f, ldf, pt, k, i);  // U(i, k) = L(k, i)
+    }
+    m[t] = mv;
+    u[t] = uv;
+  }
+}
+
+// out(perm[i], perm[j]) = (L D L^T)(i, j) = -C(min(i,j), max(i,j)).
+__global__ void rec_scatter_kernel(int n, const double* c, long long ld, const int* perm, double* out,
+                                   long long ldo) {
+  const long long total = static_cast<long long>(n) * n;
+  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int i = static_cast<int>(t / n), j = static_cast<int>(t % n);
+    const int lo = min(i, j), hi = max(i, j);
+    out[static_cast<long long>(perm[i]) * ldo + perm[j]] = -c[static_cast<long long>(lo) * ld + hi];
+  }
+}
+
+// Dense L (unit lower) and D (block diagonal) from the compact factors.
+__global__ void extract_ld_kernel(int n, const double* f, long long ldf, const int* pt, double* l, long long ldl,
+                                  double* d, long long ldd) {
   const long long total = static_cast<long long>(n) * n;
   for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < total;
        t += static_cast<long long>(gridDim.x) * blockDim.x) {
     const int i = static_cast<int>(t / n), k = static_cast<int>(t % n);
-    auto lval = [&](int row, int col) -> double {
-      if (row == col) return 1.0;
-      if (row < col) return 0.0;
-      if (pt[col] == 2 && row == col + 1) return 0.0;
-      return f[static_cast<long long>(col) * ldf + row];
-    };
-    double v;
-    if (pt[k] == 2 && k + 1 < n) {
-      v = lval(i, k) * f[k * ldf + k] + lval(i, k + 1) * f[k * ldf + k + 1];
-    } else if (pt[k] == -2 && k > 0) {
-      v = lval(i, k - 1) * f[(k - 1) * ldf + k] + lval(i, k) * f[k * ldf + k];
-    } else {
-      v = lval(i, k) * f[k * ldf + k];
+    if (l) l[static_cast<long long>(i) * ldl + k] = l_entry(f, ldf, pt, i, k);
+    if (d) {
+      double v = 0.0;
+      if (i == k) {
+        v = f[static_cast<long long>(i) * ldf + i];
+      } else if (k == i + 1 && pt[i] == 2) {
+        v = f[static_cast<long long>(i) * ldf + k];
+      } else if (i == k + 1 && pt[k] == 2) {
+        v = f[static_cast<long long>(k) * ldf + i];
+      }
+      d[static_cast<long long>(i) * ldd + k] = v;
     }
-    m[t] = v;
   }
-}
-
-// out(perm[i], perm[j]) = sum_k M(i,k) L(j,k)
-__global__ void rec_kernel(int n, const double* f, long long ldf, const int* pt, const int* perm,
-                           const double* m, double* out, long long ldo) {
-  const int i = blockIdx.y * 16 + threadIdx.y;
-  const int j = blockIdx.x * 16 + threadIdx.x;
-  if (i >= n || j >= n) return;
-  const int kmax = min(n - 1, min(i + 1, j));
-  double s = 0.0;
-  for (int k = 0; k <= kmax; ++k) {
-    double l;
-    if (j == k) {
-      l = 1.0;
-    } else if (j < k || (pt[k] == 2 && j == k + 1)) {
-      l = 0.0;
-    } else {
-      l = f[static_cast<long long>(k) * ldf + j];
-    }
-    s += m[static_cast<long long>(i) * n + k] * l;
-  }
-  out[static_cast<long long>(perm[i]) * ldo + perm[j]] = s;
 }
 
 constexpr int kMaxAttrDevices = 64;
@@ -401,15 +423,37 @@ int solve_enqueue(int n, const double* f, long long ldf, const int* perm, const 
   return BBK_OK;
 }
 
+size_t reconstruct_work_doubles(int n) {
+  const size_t ld = align_up(static_cast<size_t>(n), 128);
+  return 3 * ld * ld;
+}
+
+// P^T L D L^T P: M = L D and U = L^T formed on the device, the upper tiles
+// of M U on the FP64 tensor cores (the trailing-update tile kernels with
+// C = 0), then mirrored and permuted.  work: reconstruct_work_doubles(n).
 int reconstruct_enqueue(int n, const double* f, long long ldf, const int* perm,
-                        const int* pivot_types, double* out, long long ldo, double* m,
+                        const int* pivot_types, double* out, long long ldo, double* work,
                         cudaStream_t s) {
-  const long long total = static_cast<long long>(n) * n;
-  ld_kernel<<<grid_for(total, 256), 256, 0, s>>>(n, f, ldf, pivot_types, m);
+  const long long ld = static_cast<long long>(align_up(static_cast<size_t>(n), 128));
+  double* m = work;
+  double* u = m + ld * ld;
+  double* c = u + ld * ld;
+  BBK_CUDA_TRY(cudaMemsetAsync(c, 0, static_cast<size_t>(ld * ld) * sizeof(double), s));
+  ld_lt_kernel<<<grid_for(ld * ld, 256), 256, 0, s>>>(n, f, ldf, pivot_types, ld, m, u);
   BBK_CUDA_TRY(cudaGetLastError());
   count_launch();
-  dim3 blk(16, 16), grd((n + 15) / 16, (n + 15) / 16);
-  rec_kernel<<<grd, blk, 0, s>>>(n, f, ldf, pivot_types, perm, m, out, ldo);
+  int rc = launch_upper_product(n, m, u, ld, c, s);
+  if (rc) return rc;
+  rec_scatter_kernel<<<grid_for(static_cast<long long>(n) * n, 256), 256, 0, s>>>(n, c, ld, perm, out, ldo);
+  BBK_CUDA_TRY(cudaGetLastError());
+  count_launch();
+  return BBK_OK;
+}
+
+int extract_ld_enqueue(int n, const double* f, long long ldf, const int* pivot_types, double* l, long long ldl,
+                       double* d, long long ldd, cudaStream_t s) {
+  extract_ld_kernel<<<grid_for(static_cast<long long>(n) * n, 256), 256, 0, s>>>(n, f, ldf, pivot_types, l, ldl,
+                                                                                 d, ldd);
   BBK_CUDA_TRY(cudaGetLastError());
   count_launch();
   return BBK_OK;

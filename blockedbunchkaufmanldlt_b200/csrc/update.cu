@@ -24,6 +24,7 @@
 
 #include <algorithm>
 #include <cstdlib>
+#include <cstring>
 #include <mutex>
 #include <type_traits>
 
@@ -455,163 +456,171 @@ __global__ void __launch_bounds__(kThreadsMma) mma_update_kernel(UpdArgs U) {
 }
 
 // ---------------------------------------------------------------------------
-// FP64 tensor-core update with 128x128 C tiles (the large trailing matrices).
-// 8 warps of 64x32, k chunks of 32 in a kStagesL-deep cp.async ring that
-// runs across tile boundaries (the next tile's first chunks load while this
-// tile finishes), so the tensor pipe only waits at an epilogue.  Each C tile
-// is prefetched into L2 when its first chunk is consumed and updated straight
-// from registers (C -= acc) at its end.  Against the 64x64 tile this halves
-// the L2 operand traffic per flop (each A/B element feeds 128 instead of 64
-// outputs) and the C traffic per flop stays the same.
+// FP64 tensor-core update with wide C tiles (the large trailing matrices):
+// BM x BN tiles (BN a multiple of BM), warps of WM x WN, k chunks of 32 in a
+// Stages-deep cp.async ring that runs across tile boundaries (the next
+// tile's first chunks load while this tile finishes).  Each C tile is
+// prefetched into L2 when its first chunk is consumed and updated straight
+// from registers (C -= acc) at its end.  Every A/B element staged feeds BN
+// (resp. BM) outputs instead of 64, which cuts the operand traffic from L2
+// per flop; the C traffic per flop is the same as with 64 x 64 tiles.
+// Tiles cover the upper triangle of the trailing matrix: column block J
+// (BN wide) holds row blocks I <= (J + 1) R - 1, R = BN / BM, so the first
+// R J(J+1)/2 tiles are the column blocks before J.
 // ---------------------------------------------------------------------------
-constexpr int kBML = 128, kBNL = 128;
-constexpr int kThreadsL = 256;
-constexpr int kStagesL = 3;
-constexpr int kAPitchL = kBK + kPadA;   // A stage [128][36]: k contiguous
-constexpr int kBPitchL = kBNL + kPadB;  // B stage [32][132]: j contiguous
-constexpr int kAStageL = kBML * kAPitchL;
-constexpr int kStageL = kAStageL + kBK * kBPitchL;
-constexpr size_t kBytesL = static_cast<size_t>(kStagesL) * kStageL * sizeof(double);
-static_assert(kBytesL <= 227 * 1024, "stages must fit the shared memory of one CTA");
+template <int BM, int BN, int WM, int WN, int Stages>
+struct Wide {
+  static constexpr int kWarps = (BM / WM) * (BN / WN);
+  static constexpr int kThreads = kWarps * 32;
+  static constexpr int kR = BN / BM;
+  static constexpr int kAPitch = kBK + kPadA;  // A stage [BM][36]: k contiguous
+  static constexpr int kBPitch = BN + kPadB;   // B stage [32][BN + 4]: j contiguous
+  static constexpr int kAStage = BM * kAPitch;
+  static constexpr int kStage = kAStage + kBK * kBPitch;
+  static constexpr size_t kBytes = static_cast<size_t>(Stages) * kStage * sizeof(double);
+  static constexpr int kMT = WM / 16, kNT = WN / 8;  // m16n8k8 tiles per warp
+  static_assert(BN % BM == 0, "column blocks must cover whole row blocks");
+  static_assert(kBytes <= 227 * 1024, "stages must fit the shared memory of one CTA");
+  static_assert((BM * kBK / 2) % kThreads == 0 && (kBK * BN / 2) % kThreads == 0, "even copy split");
 
-__device__ __forceinline__ int tile_count_l(int tm) { return tm * (tm + 1) / 2; }
-
-// Chunk ch of tile (i0, j0) into stage st: A 128 x 32, B 32 x 128, 16-byte
-// copies (k >= inner zero-filled).
-__device__ __forceinline__ void load_stage_l(const UpdArgs& U, double* st, int i0, int j0, int k0) {
-  double* as = st;
-  double* bs = st + kAStageL;
-  const int t = threadIdx.x;
-#pragma unroll
-  for (int u = 0; u < (kBML * kBK / 2) / kThreadsL; ++u) {
-    const int c = t + u * kThreadsL;
-    const int ii = c / (kBK / 2), kk = (c % (kBK / 2)) * 2;
-    const int k = k0 + kk;
-    const int nvalid = max(0, min(2, U.inner - k));
-    const double* src = U.a + static_cast<long long>(i0 + ii) * U.a_si + (nvalid ? k : 0);
-    cp_async_16(&as[ii * kAPitchL + kk], src, nvalid * 8);
+  __device__ static int tiles(int tn) { return kR * tn * (tn + 1) / 2; }
+  __device__ static void origin(const UpdArgs& U, int t, int& i0, int& j0) {
+    int j = static_cast<int>((sqrt(8.0 * t / kR + 1.0) - 1.0) * 0.5);
+    while (j > 0 && kR * j * (j + 1) / 2 > t) --j;
+    while (kR * (j + 1) * (j + 2) / 2 <= t) ++j;
+    i0 = U.tile_i0 + (t - kR * j * (j + 1) / 2) * BM;
+    j0 = U.tile_i0 + j * BN;
   }
+  // chunk at k0 of tile (i0, j0) into stage st (k >= inner zero-filled)
+  __device__ static void load(const UpdArgs& U, double* st, int i0, int j0, int k0) {
+    double* as = st;
+    double* bs = st + kAStage;
+    const int t = threadIdx.x;
 #pragma unroll
-  for (int u = 0; u < (kBK * kBNL / 2) / kThreadsL; ++u) {
-    const int c = t + u * kThreadsL;
-    const int kk = c / (kBNL / 2), jj = (c % (kBNL / 2)) * 2;
-    const int k = k0 + kk;
-    const bool ok = k < U.inner;
-    const double* src = U.b + static_cast<long long>(ok ? k : 0) * U.b_sk + j0 + jj;
-    cp_async_16(&bs[kk * kBPitchL + jj], src, ok ? 16 : 0);
+    for (int u = 0; u < (BM * kBK / 2) / kThreads; ++u) {
+      const int c = t + u * kThreads;
+      const int ii = c / (kBK / 2), kk = (c % (kBK / 2)) * 2;
+      const int k = k0 + kk;
+      const int nvalid = max(0, min(2, U.inner - k));
+      const double* src = U.a + static_cast<long long>(i0 + ii) * U.a_si + (nvalid ? k : 0);
+      cp_async_16(&as[ii * kAPitch + kk], src, nvalid * 8);
+    }
+#pragma unroll
+    for (int u = 0; u < (kBK * BN / 2) / kThreads; ++u) {
+      const int c = t + u * kThreads;
+      const int kk = c / (BN / 2), jj = (c % (BN / 2)) * 2;
+      const int k = k0 + kk;
+      const bool ok = k < U.inner;
+      const double* src = U.b + static_cast<long long>(ok ? k : 0) * U.b_sk + j0 + jj;
+      cp_async_16(&bs[kk * kBPitch + jj], src, ok ? 16 : 0);
+    }
   }
-}
+};
 
-__device__ __forceinline__ void tile_origin_l(const UpdArgs& U, int t, int& i0, int& j0) {
-  int j = static_cast<int>((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
-  while (j * (j + 1) / 2 > t) --j;
-  while ((j + 1) * (j + 2) / 2 <= t) ++j;
-  i0 = U.tile_i0 + (t - j * (j + 1) / 2) * kBML;
-  j0 = U.tile_i0 + j * kBNL;
-}
-
-__global__ void __launch_bounds__(kThreadsL, 1) mma_update_large_kernel(UpdArgs U) {
+template <int BM, int BN, int WM, int WN, int Stages>
+__global__ void __launch_bounds__(Wide<BM, BN, WM, WN, Stages>::kThreads)
+    mma_update_wide_kernel(UpdArgs U) {
+  using W = Wide<BM, BN, WM, WN, Stages>;
   extern __shared__ double smem[];
   if (U.st != nullptr) {
-    // panel mode: range from the device state, tiles of 128 from the
-    // 128-aligned row at or below the trailing matrix's first row
+    // panel mode: range from the device state, tiles from the BN-aligned
+    // row at or below the trailing matrix's first row
     if (ld_relaxed_s32(&U.st->abort)) return;
     const int k0 = ldcg(&U.st->kstart[U.panel & 1]);
     const int e = ldcg(&U.st->kstart[(U.panel + 1) & 1]);
     U.inner = e - k0;
     U.i_lo = U.j_lo = e;
     U.i_hi = U.j_hi = U.n;
-    U.tile_i0 = U.tile_j0 = (e / kBML) * kBML;
+    U.tile_i0 = U.tile_j0 = (e / BN) * BN;
     if (U.inner <= 0 || e >= U.n) return;
   }
-  const int tm = (U.n - U.tile_i0 + kBML - 1) / kBML;
-  const int ntiles = tile_count_l(tm);
+  const int tn = (U.n - U.tile_i0 + BN - 1) / BN;
+  const int ntiles = W::tiles(tn);
   if (static_cast<int>(blockIdx.x) >= ntiles) return;
   const int nchunks = (U.inner + kBK - 1) / kBK;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = lane >> 2, tq = lane & 3;
-  const int wm = (warp >> 2) * 64, wn = (warp & 3) * 32;
+  const int wm = (warp / (BN / WN)) * WM, wn = (warp % (BN / WN)) * WN;
   // (tile, chunk) items of this CTA, in order: tiles blockIdx.x + m * gridDim.x
   const int my_tiles = (ntiles - static_cast<int>(blockIdx.x) + static_cast<int>(gridDim.x) - 1) /
                        static_cast<int>(gridDim.x);
   const long long items = static_cast<long long>(my_tiles) * nchunks;
-  // loader cursor (item ld_item = tile ld_tile, chunk ld_ch)
-  long long ld_item = 0;
+  long long ld_item = 0;  // loader cursor: item ld_item = tile ld_m, chunk ld_ch
   int ld_ch = 0, ld_m = 0, ld_i0 = 0, ld_j0 = 0;
-  tile_origin_l(U, blockIdx.x, ld_i0, ld_j0);
+  W::origin(U, blockIdx.x, ld_i0, ld_j0);
   auto issue = [&]() {
     if (ld_item < items) {
-      load_stage_l(U, smem + static_cast<size_t>(ld_item % kStagesL) * kStageL, ld_i0, ld_j0, ld_ch * kBK);
+      W::load(U, smem + static_cast<size_t>(ld_item % Stages) * W::kStage, ld_i0, ld_j0, ld_ch * kBK);
       ++ld_item;
       if (++ld_ch == nchunks) {
         ld_ch = 0;
         ++ld_m;
         if (ld_m < my_tiles)
-          tile_origin_l(U, static_cast<int>(blockIdx.x) + ld_m * static_cast<int>(gridDim.x), ld_i0, ld_j0);
+          W::origin(U, static_cast<int>(blockIdx.x) + ld_m * static_cast<int>(gridDim.x), ld_i0, ld_j0);
       }
     }
     cp_async_commit();  // one group per item slot, empty past the end
   };
 #pragma unroll
-  for (int s = 0; s < kStagesL - 1; ++s) issue();
+  for (int s = 0; s < Stages - 1; ++s) issue();
 
   long long item = 0;
   for (int m = 0; m < my_tiles; ++m) {
     int i0, j0;
-    tile_origin_l(U, static_cast<int>(blockIdx.x) + m * static_cast<int>(gridDim.x), i0, j0);
+    W::origin(U, static_cast<int>(blockIdx.x) + m * static_cast<int>(gridDim.x), i0, j0);
     // the C tile's rows go to L2 now; the epilogue reads them after the k loop
-    for (int r = threadIdx.x >> 3; r < kBML; r += kThreadsL / 8) {
+    for (int r = threadIdx.x / (BN / 16); r < BM; r += W::kThreads / (BN / 16)) {
       const int i = i0 + r;
-      const int jc = j0 + (threadIdx.x & 7) * 16;
+      const int jc = j0 + (threadIdx.x % (BN / 16)) * 16;
       if (i >= U.i_lo && i < U.i_hi && jc < U.j_hi && i <= jc + 15)
         asm volatile("prefetch.global.L2 [%0];" ::"l"(U.c + static_cast<long long>(i) * U.ldc + jc));
     }
-    double acc[4][4][4];
+    double acc[W::kMT][W::kNT][4];
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+    for (int a = 0; a < W::kMT; ++a)
 #pragma unroll
-      for (int b = 0; b < 4; ++b)
+      for (int b = 0; b < W::kNT; ++b)
 #pragma unroll
         for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.0;
     for (int ch = 0; ch < nchunks; ++ch, ++item) {
-      cp_async_wait<kStagesL - 2>();
+      cp_async_wait<Stages - 2>();
       __syncthreads();  // item's stage has landed; every warp is done with the stage refilled next
       issue();
-      const double* as = smem + static_cast<size_t>(item % kStagesL) * kStageL;
-      const double* bs = as + kAStageL;
+      const double* as = smem + static_cast<size_t>(item % Stages) * W::kStage;
+      const double* bs = as + W::kAStage;
 #pragma unroll
       for (int ks = 0; ks < kBK; ks += 8) {
-        double af[4][4], bf[4][2];
+        double af[W::kMT][4], bf[W::kNT][2];
 #pragma unroll
-        for (int mt = 0; mt < 4; ++mt) {
+        for (int mt = 0; mt < W::kMT; ++mt) {
           const int r = wm + mt * 16 + g;
-          af[mt][0] = as[r * kAPitchL + ks + tq];
-          af[mt][1] = as[(r + 8) * kAPitchL + ks + tq];
-          af[mt][2] = as[r * kAPitchL + ks + tq + 4];
-          af[mt][3] = as[(r + 8) * kAPitchL + ks + tq + 4];
+          af[mt][0] = as[r * W::kAPitch + ks + tq];
+          af[mt][1] = as[(r + 8) * W::kAPitch + ks + tq];
+          af[mt][2] = as[r * W::kAPitch + ks + tq + 4];
+          af[mt][3] = as[(r + 8) * W::kAPitch + ks + tq + 4];
         }
 #pragma unroll
-        for (int nt = 0; nt < 4; ++nt) {
+        for (int nt = 0; nt < W::kNT; ++nt) {
           const int col = wn + nt * 8 + g;
-          bf[nt][0] = bs[(ks + tq) * kBPitchL + col];
-          bf[nt][1] = bs[(ks + tq + 4) * kBPitchL + col];
+          bf[nt][0] = bs[(ks + tq) * W::kBPitch + col];
+          bf[nt][1] = bs[(ks + tq + 4) * W::kBPitch + col];
         }
 #pragma unroll
-        for (int mt = 0; mt < 4; ++mt)
+        for (int mt = 0; mt < W::kMT; ++mt)
 #pragma unroll
-          for (int nt = 0; nt < 4; ++nt) mma_16x8x8(acc[mt][nt], af[mt], bf[nt]);
+          for (int nt = 0; nt < W::kNT; ++nt) mma_16x8x8(acc[mt][nt], af[mt], bf[nt]);
       }
     }
     // C -= acc on the tile's valid part (upper triangle of the trailing matrix)
 #pragma unroll
-    for (int mt = 0; mt < 4; ++mt) {
+    for (int mt = 0; mt < W::kMT; ++mt) {
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int i = i0 + wm + mt * 16 + g + h * 8;
         if (i < U.i_lo || i >= U.i_hi) continue;
         double* crow = U.c + static_cast<long long>(i) * U.ldc;
 #pragma unroll
-        for (int nt = 0; nt < 4; ++nt) {
+        for (int nt = 0; nt < W::kNT; ++nt) {
           const int j = j0 + wn + nt * 8 + tq * 2;
           const double v0 = acc[mt][nt][h * 2], v1 = acc[mt][nt][h * 2 + 1];
           const bool ok0 = j >= U.j_lo && j < U.j_hi && (!U.upper_only || i <= j);
@@ -631,6 +640,12 @@ __global__ void __launch_bounds__(kThreadsL, 1) mma_update_large_kernel(UpdArgs 
   }
   cp_async_wait<0>();
 }
+
+// The wide-tile configurations: 128 x 128 (8 warps of 64 x 32, 3 stages,
+// one CTA per SM) and 64 x 128 (4 warps of 32 x 64, 2 stages, two CTAs per
+// SM so one CTA's barrier waits and epilogue overlap the other's MMAs).
+using WideSquare = Wide<128, 128, 64, 32, 3>;
+using WideHalf = Wide<64, 128, 32, 64, 2>;
 
 // ---------------------------------------------------------------------------
 // SIMT tiles: reference-ordered FP64 and FP32.  256 threads, 4x4 per thread.
@@ -724,14 +739,56 @@ bool use_k16() {
   return v;
 }
 
-// 128x128 tiles for large trailing matrices (BBK_UPDATE_LARGE_TILES=0
-// keeps the 64x64 kernel everywhere: tuning and comparison).
-bool use_large_tiles() {
-  static const bool v = [] {
-    const char* e = getenv("BBK_UPDATE_LARGE_TILES");
-    return e ? atoi(e) != 0 : true;
+// Tile shape of the FP64 tensor-core update for large trailing matrices:
+// BBK_UPDATE_TILE = 64 (64 x 64 everywhere), 128 (128 x 128) or 64x128.
+int wide_tile_choice() {
+  static const int v = [] {
+    const char* e = getenv("BBK_UPDATE_TILE");
+    if (!e) return 0;
+    if (std::strcmp(e, "128") == 0) return 1;
+    if (std::strcmp(e, "64x128") == 0) return 2;
+    return 0;
   }();
   return v;
+}
+
+// Launches the wide-tile kernel `choice` (1: 128 x 128, 2: 64 x 128) for U
+// when its upper triangle has at least two tiles per resident CTA; returns
+// false (nothing launched) otherwise.
+int launch_wide(const UpdArgs& U, int choice, long long order, bool* launched, cudaStream_t s) {
+  *launched = false;
+  const int sms = device_sm_count();
+  const long long tn = (order + 127) / 128;
+  const int per_sm = choice == 1 ? 1 : 2;
+  const long long tiles = (choice == 1 ? 1 : 2) * tn * (tn + 1) / 2;
+  if (choice == 0 || tiles < 2LL * per_sm * sms) return BBK_OK;
+  static std::once_flag attr_once[2][64];
+  int dev = 0;
+  BBK_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return set_error(BBK_ERR_NO_DEVICE, "device %d out of range", dev);
+  cudaError_t attr_err = cudaSuccess;
+  const int grid = static_cast<int>(std::min<long long>(tiles, static_cast<long long>(per_sm) * sms));
+  if (choice == 1) {
+    auto fn = mma_update_wide_kernel<128, 128, 64, 32, 3>;
+    std::call_once(attr_once[0][dev], [&] {
+      attr_err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(WideSquare::kBytes));
+    });
+    BBK_CUDA_TRY(attr_err);
+    fn<<<grid, WideSquare::kThreads, WideSquare::kBytes, s>>>(U);
+  } else {
+    auto fn = mma_update_wide_kernel<64, 128, 32, 64, 2>;
+    std::call_once(attr_once[1][dev], [&] {
+      attr_err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(WideHalf::kBytes));
+    });
+    BBK_CUDA_TRY(attr_err);
+    fn<<<grid, WideHalf::kThreads, WideHalf::kBytes, s>>>(U);
+  }
+  BBK_CUDA_TRY(cudaGetLastError());
+  count_launch();
+  *launched = true;
+  return BBK_OK;
 }
 
 template <bool kAK, bool kVec>
@@ -1135,30 +1192,41 @@ int launch_update(const FactorPlan& plan, int panel, cudaStream_t s) {
                ? launch_bf16_split<1>(U, buf, plan.kpad, plan.hstride, grid_mma, vec, s)
                : launch_bf16_split<3>(U, buf, plan.kpad, plan.hstride, grid_mma, vec, s);
   }
-  if (plan.mode == BBK_UPDATE_FP64 && vec && use_large_tiles()) {
-    // 128x128 tiles while the trailing matrix gives every SM at least two of
-    // them (the grid is persistent, one CTA per SM)
-    const long long tml = (plan.n - (nominal_e / kBML) * kBML + kBML - 1) / kBML;
-    const long long tiles_l = tml * (tml + 1) / 2;
-    if (tiles_l >= 2LL * sms) {
-      static std::once_flag attr_once[64];
-      int dev = 0;
-      BBK_CUDA_TRY(cudaGetDevice(&dev));
-      if (dev < 0 || dev >= 64) return set_error(BBK_ERR_NO_DEVICE, "device %d out of range", dev);
-      cudaError_t attr_err = cudaSuccess;
-      std::call_once(attr_once[dev], [&] {
-        attr_err = cudaFuncSetAttribute(mma_update_large_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        static_cast<int>(kBytesL));
-      });
-      BBK_CUDA_TRY(attr_err);
-      const int grid = static_cast<int>(std::min<long long>(tiles_l, sms));
-      mma_update_large_kernel<<<grid, kThreadsL, kBytesL, s>>>(U);
-      BBK_CUDA_TRY(cudaGetLastError());
-      count_launch();
-      return BBK_OK;
-    }
+  if (plan.mode == BBK_UPDATE_FP64 && vec) {
+    bool launched = false;
+    const int rc = launch_wide(U, wide_tile_choice(), plan.n - nominal_e, &launched, s);
+    if (rc || launched) return rc;
   }
   return launch_by_mode(U, plan.mode, true, vec, grid_mma, grid_simt, s);
+}
+
+// C(i, j) -= sum_k M(i, k) U(k, j) on the upper tiles (i <= j) of an n x n
+// product, all three row-major with leading dimension ld (even, >= the
+// order rounded up to 128, rows up to that bound readable): the
+// reconstruction P^T L D L^T P runs this with M = L D, U = L^T and C = 0.
+int launch_upper_product(int n, const double* m, const double* u, long long ld, double* c, cudaStream_t s) {
+  UpdArgs U{};
+  U.a = m;
+  U.a_si = ld;
+  U.a_sk = 1;
+  U.b = u;
+  U.b_sk = ld;
+  U.c = c;
+  U.ldc = ld;
+  U.i_lo = U.j_lo = 0;
+  U.i_hi = U.j_hi = n;
+  U.inner = n;
+  U.upper_only = 1;
+  U.triangular = 1;
+  U.tile_i0 = U.tile_j0 = 0;
+  U.n = n;
+  const int sms = device_sm_count();
+  bool launched = false;
+  const int rc = launch_wide(U, wide_tile_choice(), n, &launched, s);
+  if (rc || launched) return rc;
+  U.tiles_m = U.tiles_n = (n + kBM - 1) / kBM;
+  const long long tiles = static_cast<long long>(U.tiles_m) * (U.tiles_m + 1) / 2;
+  return launch_mma<true, true>(U, static_cast<int>(std::max(1LL, std::min<long long>(tiles, 3LL * sms))), s);
 }
 
 int launch_update_block(int rows, int cols, int inner, const double* left, int ls,

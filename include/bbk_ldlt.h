@@ -133,22 +133,36 @@ int bbk_factor_device_async(int n, int block_size, double* a, long long lda,
                             int update_mode, void* workspace,
                             size_t workspace_bytes, int* status_device,
                             void* stream);
-/* Diagnostics for pivot-sequence comparisons: bbk_factor_device_async that
- * also records what every Bunch-Kaufman decision compared, so a decision
- * that another summation order could flip (a near-tie) can be recognised.
- * pivot_log (device, 4 * n doubles) receives, at the factored position p
- * where each pivot step's pivot starts: |W(p,p)| (tested against alpha *
- * omega, src/block_ldlt_decomposition.cc:90-92), omega = max_{j>p} |W(p,j)|
- * (FindCurrentRowMax, :164-182), sigma = max_{i>=p, i!=r} |W(i,r)| and
- * |W(r,r)| (FindCandidateColumnMax and SelectPivot, :354-390; NaN when the
- * first test kept the 1x1 pivot).  Every other entry is NaN (the second row
- * of a 2x2 pivot).  The reference has no such log; the bench and the parity
- * tests use it. */
-int bbk_factor_device_logged(int n, int block_size, double* a, long long lda,
-                             int* perm, int* pivot_types, int* panel_end,
-                             int update_mode, double* pivot_log,
-                             void* workspace, size_t workspace_bytes,
-                             int* status_device, void* stream);
+/* Optional outputs of bbk_factor_device_ex (no reference entry point: the
+ * reference keeps both inside its object).  Any pointer may be NULL.
+ *
+ * pivot_log (device, 4 * n doubles): what every Bunch-Kaufman decision
+ *   compared, so a decision that another summation order could flip (a
+ *   near-tie) can be recognised.  At the factored position p where each
+ *   pivot step's pivot starts: |W(p,p)| (tested against alpha * omega,
+ *   src/block_ldlt_decomposition.cc:90-92), omega = max_{j>p} |W(p,j)|
+ *   (FindCurrentRowMax, :164-182), sigma = max_{i>=p, i!=r} |W(i,r)| and
+ *   |W(r,r)| (FindCandidateColumnMax and SelectPivot, :354-390; NaN when the
+ *   first test kept the 1x1 pivot).  Every other entry is NaN (the second
+ *   row of a 2x2 pivot).
+ * workspace_rows (device, n x workspace_ld row-major): each panel's
+ *   workspace rows W = D U (the unscaled updated pivot rows) at the columns
+ *   the trailing update reads, i.e. W(p, j) for the panel's rows p and
+ *   j >= the panel's end, in the column order at the panel's end -- the
+ *   contents of the reference's Workspace() outside its diagonal blocks
+ *   (written by FactorPanel, :80-120, and read by UpdateTrailingBlocks,
+ *   :706-744).  Nothing else of the array is written. */
+typedef struct bbk_factor_extras {
+  double* pivot_log;
+  double* workspace_rows;
+  long long workspace_ld;
+} bbk_factor_extras;
+/* bbk_factor_device_async with the optional outputs above. */
+int bbk_factor_device_ex(int n, int block_size, double* a, long long lda,
+                         int* perm, int* pivot_types, int* panel_end,
+                         int update_mode, const bbk_factor_extras* extras,
+                         void* workspace, size_t workspace_bytes,
+                         int* status_device, void* stream);
 /* Host variant: a (n x lda, in/out), perm, pivot_types, panel_end are host
  * memory.  Copies in, factors on the current device, copies out. */
 int bbk_factor_host(int n, int block_size, double* a, long long lda,
@@ -240,10 +254,40 @@ int bbk_factor_solve_host(int n, int block_size, double* a, long long lda,
 /* ---- reconstruction (reference ReconstructOriginal,
  * src/block_ldlt_decomposition.cc:61-78) --------------------------------
  * out (n x ldo row-major, full) = P^T L D L^T P from compact factors.
- * Device pointers. */
+ * M = L D and L^T are formed on the device and the upper triangle of their
+ * product runs on the FP64 tensor cores (the trailing-update tile kernels);
+ * the result is mirrored and permuted.  Temporary device memory: 3 x ld^2
+ * doubles, ld = n rounded up to 128.  Device pointers. */
 int bbk_reconstruct_device(int n, const double* factors, long long ldf,
                            const int* perm, const int* pivot_types,
                            double* out, long long ldo, void* stream);
+/* ExtractRegularFactorsFromCompact (src/block_ldlt_decomposition.cc:746-763)
+ * on the device: dense L (n x ldl row-major, unit lower: L(i,k) = F(k,i)
+ * for i > k, except the coupling entry of a 2x2 pivot) and D (n x ldd,
+ * block diagonal: F(k,k), and F(k,k+1) at (k,k+1) and (k+1,k) of a 2x2),
+ * the kFull mode's LFactor() / DFactor().  Either output may be NULL.
+ * Device pointers; waits for `stream`. */
+int bbk_extract_ld_device(int n, const double* factors, long long ldf,
+                          const int* pivot_types, double* l, long long ldl,
+                          double* d, long long ldd, void* stream);
+
+/* ---- sampled residual (the reference's large-matrix check,
+ * tests/block_ldlt_large_stress_test.cc:160-244) -------------------------
+ * For `count` sampled entries (rows[k], cols[k]) of the original matrix `a`
+ * (upper triangle read, lda), the same entry of P^T L D L^T P computed
+ * straight from the compact factors, without forming L D L^T; *residual
+ * (host) = sqrt(sum (reconstructed - original)^2) / max(sqrt(sum original^2),
+ * 1).  Every sample is summed over the pivots in the reference's order with
+ * each product and sum rounded separately, and the sums run in sample
+ * order, so equal factors give the reference's value bit for bit.  rows and
+ * cols are device int arrays; a, factors, perm, pivot_types device memory.
+ * A sample outside [0, n) or a perm that is not a permutation makes the
+ * result NaN.  Waits for `stream`. */
+int bbk_sampled_residual_device(int n, const double* a, long long lda,
+                                const double* factors, long long ldf,
+                                const int* perm, const int* pivot_types,
+                                int count, const int* rows, const int* cols,
+                                double* residual, void* stream);
 
 /* ---- the reference's kernel boundary (include/kernels.h:6-23,
  * src/kernels.cc:11-91), device pointers, element strides -------------- */

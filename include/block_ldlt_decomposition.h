@@ -7,6 +7,7 @@
 #ifndef NAIVE_BLOCK_LDLT_BLOCK_LDLT_DECOMPOSITION_H_
 #define NAIVE_BLOCK_LDLT_BLOCK_LDLT_DECOMPOSITION_H_
 
+#include <memory>
 #include <vector>
 
 #include "block_matrix.h"
@@ -30,8 +31,11 @@ class BlockLdltDecomposition {
   const RegularMatrix& LFactor() const { return l_factor_; }
   const RegularMatrix& DFactor() const { return d_factor_; }
   const BlockMatrix& CompactFactors() const { return factors_; }
-  // Same geometry as CompactFactors(); its values are not produced (the
-  // workspace rows stay on the GPU) and read as zero.
+  // Same geometry as CompactFactors().  Outside the diagonal blocks it holds,
+  // like the reference's, each panel's workspace rows W = D U (the unscaled
+  // updated pivot rows the trailing update reads) in the column order at the
+  // panel's end; the diagonal blocks, where the reference also keeps
+  // intermediate candidate copies, read as zero.
   const BlockMatrix& Workspace() const { return workspace_; }
   const std::vector<int>& Permutation() const { return permutation_; }
   const std::vector<int>& PivotTypes() const { return pivot_types_; }
@@ -45,6 +49,7 @@ class BlockLdltDecomposition {
   std::vector<double> Solve(const std::vector<double>& b, int nrhs = 1) const;
 
  private:
+  struct DeviceFactors;  // the compact factors, permutation and pivot types on the GPU
   void RebuildGeometry(BlockMatrix* matrix, const std::vector<int>& panel_end) const;
 
   RegularMatrix original_;
@@ -54,7 +59,9 @@ class BlockLdltDecomposition {
   RegularMatrix d_factor_;
   std::vector<int> permutation_;
   std::vector<int> pivot_types_;
-  std::vector<double> dense_;  // compact factors, n x n row-major (upper)
+  // after Factorize(): the device copy Solve() and ReconstructOriginal() use
+  // (shared by copies of this object; never modified after Factorize())
+  std::shared_ptr<const DeviceFactors> device_;
   FactorizationMode mode_ = FactorizationMode::kFull;
   int update_mode_ = 0;
   bool factorized_ = false;

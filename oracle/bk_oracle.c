@@ -62,7 +62,7 @@ static void symmetric_move(double* a, long long lda, int n, int s, int r,
  * roundings each accumulator sees is unchanged, so results are too. */
 static int factor_impl(int n, int b, double* a, long long lda, int* perm,
                        int* pivot_types, int* panel_end, int* shifted,
-                       int max_panels, double* log) {
+                       int max_panels, double* log, double* w_out) {
   if (n <= 0 || b <= 0 || lda < n || !a || !perm || !pivot_types) return -1;
   const int nb = (n + b - 1) / b;
   double* w = (double*)calloc((size_t)(b + 1) * (size_t)n, sizeof(double));
@@ -229,6 +229,9 @@ static int factor_impl(int n, int b, double* a, long long lda, int* perm,
     const int e = p; /* first row after this panel */
     if (panel_end) panel_end[panel] = e;
     if (shifted) shifted[panel] = did_shift;
+    if (w_out) /* the panel's W rows at the columns the trailing update reads */
+      for (int q = k0; q < e; ++q)
+        for (int j = e; j < n; ++j) w_out[IDX(q, j, n)] = w[IDX(q - k0, j, n)];
 
     /* UpdateTrailingBlocks (:706-744) + kernels::UpdateTrailingBlock
      * (kernels.cc:67-91): A[i,j] -= sum_q U[q,i] W[q,j] over the trailing
@@ -257,15 +260,15 @@ static int factor_impl(int n, int b, double* a, long long lda, int* perm,
 int bko_factor(int n, int block_size, double* a, long long lda, int* perm,
                int* pivot_types, int* panel_end, int* shifted) {
   const int r = factor_impl(n, block_size, a, lda, perm, pivot_types,
-                            panel_end, shifted, 1 << 30, NULL);
+                            panel_end, shifted, 1 << 30, NULL, NULL);
   return r < 0 ? -1 : 0;
 }
 
 int bko_factor_logged(int n, int block_size, double* a, long long lda,
                       int* perm, int* pivot_types, int* panel_end,
-                      int* shifted, double* log) {
+                      int* shifted, double* log, double* w_out) {
   const int r = factor_impl(n, block_size, a, lda, perm, pivot_types,
-                            panel_end, shifted, 1 << 30, log);
+                            panel_end, shifted, 1 << 30, log, w_out);
   return r < 0 ? -1 : 0;
 }
 
@@ -273,7 +276,7 @@ int bko_factor_panels(int n, int block_size, double* a, long long lda,
                       int* perm, int* pivot_types, int* panel_end,
                       int* shifted, int max_panels) {
   return factor_impl(n, block_size, a, lda, perm, pivot_types, panel_end,
-                     shifted, max_panels, NULL);
+                     shifted, max_panels, NULL, NULL);
 }
 
 void bko_scale_one_by_one(int count, double pivot, const double* source,
@@ -413,4 +416,45 @@ void bko_reconstruct(int n, const double* f, long long ldf, const int* perm,
   }
   free(m);
   free(l);
+}
+
+/* tests/block_ldlt_large_stress_test.cc:160-172 (CompactLValue) */
+static double compact_l(const double* f, long long ldf, const int* pt, int row, int col) {
+  if (row == col) return 1.0;
+  if (row < col) return 0.0;
+  if (pt[col] == 2 && row == col + 1) return 0.0;
+  return f[IDX(col, row, ldf)];
+}
+
+double bko_sampled_residual(int n, const double* a, long long lda, const double* f, long long ldf,
+                            const int* perm, const int* pt, int count, const int* rows,
+                            const int* cols) {
+  int* inv = (int*)malloc((size_t)n * sizeof(int));
+  if (!inv) return NAN;
+  for (int i = 0; i < n; ++i) inv[perm[i]] = i; /* InversePermutation, :196-202 */
+  double residual_squared = 0.0, original_squared = 0.0;
+  for (int k = 0; k < count; ++k) { /* SampledRelativeResidual, :220-244 */
+    const int r = inv[rows[k]], c = inv[cols[k]];
+    double value = 0.0; /* ReconstructedPermutedEntry, :174-194 */
+    for (int p = 0; p < n; ++p) {
+      const double row_left = compact_l(f, ldf, pt, r, p);
+      const double col_left = compact_l(f, ldf, pt, c, p);
+      value += row_left * f[IDX(p, p, ldf)] * col_left;
+      if (pt[p] == 2) {
+        const double off = f[IDX(p, p + 1, ldf)];
+        const double row_next = compact_l(f, ldf, pt, r, p + 1);
+        const double col_next = compact_l(f, ldf, pt, c, p + 1);
+        value += off * (row_left * col_next + row_next * col_left);
+      }
+    }
+    const int lo = rows[k] < cols[k] ? rows[k] : cols[k];
+    const int hi = rows[k] < cols[k] ? cols[k] : rows[k];
+    const double expected = a[IDX(lo, hi, lda)];
+    const double difference = value - expected;
+    residual_squared += difference * difference;
+    original_squared += expected * expected;
+  }
+  free(inv);
+  const double on = sqrt(original_squared);
+  return sqrt(residual_squared) / (on < 1.0 ? 1.0 : on);
 }

@@ -51,11 +51,14 @@ int bko_factor(int n, int block_size, double* a, long long lda, int* perm,
  *   [4] |W(r,r)|                         (NaN when no candidate was needed)
  * From these, every comparison of FactorPanel (:90-92) and SelectPivot
  * (:369-390) and its margin can be recomputed, so a decision that another
- * summation order could flip (a near-tie) is visible. */
+ * summation order could flip (a near-tie) is visible.  `log` may be NULL.
+ * w_out (n x n row-major, may be NULL) receives each panel's workspace rows
+ * at the columns its trailing update reads (rows of the panel, columns from
+ * the panel's end on); nothing else of it is written. */
 #define BKO_LOG_WORDS 5
 int bko_factor_logged(int n, int block_size, double* a, long long lda,
                       int* perm, int* pivot_types, int* panel_end,
-                      int* shifted, double* log);
+                      int* shifted, double* log, double* w_out);
 
 /* Same factorization, but stops after `max_panels` panels (used to time a
  * bounded sample of a large factorization).  Returns the number of panels
@@ -117,6 +120,15 @@ void bko_ref_random_block_fill(int n, int block_size, int seed, double scale,
  * (tests/block_ldlt_large_stress_test.cc:204-218): writes `count` (row, col)
  * pairs into rows/cols. */
 void bko_ref_residual_samples(int n, int seed, int count, int* rows, int* cols);
+
+/* The stress test's SampledRelativeResidual (tests/block_ldlt_large_stress_
+ * test.cc:160-244): for each sample (rows[k], cols[k]) of the original
+ * matrix `a` (upper triangle read), the same entry of P^T L D L^T P from the
+ * compact factors (CompactLValue / ReconstructedPermutedEntry, summed over
+ * every pivot in order), then sqrt(sum diff^2) / max(sqrt(sum a^2), 1). */
+double bko_sampled_residual(int n, const double* a, long long lda, const double* f,
+                            long long ldf, const int* perm, const int* pt,
+                            int count, const int* rows, const int* cols);
 
 #ifdef __cplusplus
 }

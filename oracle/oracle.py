@@ -67,8 +67,11 @@ class Port:
                                           ctypes.c_int]
         lib.bko_factor_panels.restype = ctypes.c_int
         lib.bko_factor_logged.argtypes = [ctypes.c_int, ctypes.c_int, _dp, ctypes.c_longlong,
-                                          _ip, _ip, _ip, _ip, _dp]
+                                          _ip, _ip, _ip, _ip, _dp, _dp]
         lib.bko_factor_logged.restype = ctypes.c_int
+        lib.bko_sampled_residual.argtypes = [ctypes.c_int, _dp, ctypes.c_longlong, _dp, ctypes.c_longlong,
+                                             _ip, _ip, ctypes.c_int, _ip, _ip]
+        lib.bko_sampled_residual.restype = ctypes.c_double
         lib.bko_solve.argtypes = [ctypes.c_int, _dp, ctypes.c_longlong, _ip, _ip,
                                   ctypes.c_int, _dp, ctypes.c_longlong]
         lib.bko_reconstruct.argtypes = [ctypes.c_int, _dp, ctypes.c_longlong, _ip, _ip, _dp]
@@ -112,10 +115,12 @@ class Port:
 
     LOG_WORDS = 5  # BKO_LOG_WORDS
 
-    def factor_logged(self, a: np.ndarray, block_size: int):
+    def factor_logged(self, a: np.ndarray, block_size: int, workspace_rows: bool = False):
         """factor() plus the decision log of bko_factor_logged: an n x 5
         array (|W(p,p)|, omega, runner-up of the row argmax, sigma, |W(r,r)|)
-        at every position where a pivot step started, NaN elsewhere."""
+        at every position where a pivot step started, NaN elsewhere.  With
+        workspace_rows, returns (factorization, log, W) where W (n x n, zero
+        elsewhere) holds each panel's W rows at its trailing columns."""
         n = a.shape[0]
         f = np.ascontiguousarray(a, dtype=np.float64).copy()
         perm = np.zeros(n, np.int32)
@@ -124,10 +129,13 @@ class Port:
         pe = np.zeros(nb, np.int32)
         sh = np.zeros(nb, np.int32)
         log = np.zeros((n, self.LOG_WORDS))
+        w = np.zeros((n, n)) if workspace_rows else None
         rc = self.lib.bko_factor_logged(n, block_size, _ptr(f), n, _ptr(perm, _ip), _ptr(pt, _ip),
-                                        _ptr(pe, _ip), _ptr(sh, _ip), _ptr(log))
+                                        _ptr(pe, _ip), _ptr(sh, _ip), _ptr(log), _ptr(w))
         if rc != 0:
             raise ValueError("oracle factorization rejected its arguments")
+        if workspace_rows:
+            return Factorization(f, perm, pt, pe, sh), log, w
         return Factorization(f, perm, pt, pe, sh), log
 
     def solve(self, f: Factorization, b: np.ndarray) -> np.ndarray:
@@ -159,6 +167,17 @@ class Port:
         out = np.zeros((n, n))
         self.lib.bko_ref_random_block_fill(n, block_size, seed, scale, _ptr(out))
         return out
+
+    def sampled_residual(self, a: np.ndarray, f: Factorization, rows, cols) -> float:
+        """The reference stress test's SampledRelativeResidual on compact factors."""
+        n = a.shape[0]
+        aa = np.ascontiguousarray(a, np.float64)
+        ff = np.ascontiguousarray(f.factors, np.float64)
+        r = np.ascontiguousarray(rows, np.int32)
+        c = np.ascontiguousarray(cols, np.int32)
+        return float(self.lib.bko_sampled_residual(n, _ptr(aa), n, _ptr(ff), n, _ptr(f.perm, _ip),
+                                                   _ptr(f.pivot_types, _ip), len(r), _ptr(r, _ip),
+                                                   _ptr(c, _ip)))
 
     def residual_samples(self, n: int, seed: int, count: int = 4096):
         rows = np.zeros(count, np.int32)
@@ -203,6 +222,9 @@ class Reference:
         lib.ref_factor.argtypes = [ctypes.c_int, ctypes.c_int, _dp, ctypes.c_longlong,
                                    _dp, ctypes.c_longlong, _ip, _ip, _ip, _dp]
         lib.ref_factor.restype = ctypes.c_int
+        lib.ref_factor_workspace.argtypes = [ctypes.c_int, ctypes.c_int, _dp, ctypes.c_longlong, _dp,
+                                             ctypes.c_longlong]
+        lib.ref_factor_workspace.restype = ctypes.c_int
         lib.ref_factor_full.argtypes = [ctypes.c_int, ctypes.c_int, _dp,
                                         ctypes.c_longlong, _dp, _dp, _dp]
         lib.ref_factor_full.restype = ctypes.c_int
@@ -240,6 +262,16 @@ class Reference:
         if rc != 0:
             raise RuntimeError("reference factorization threw")
         return Factorization(out, perm, pt, geometry=geo, seconds=secs.value)
+
+    def workspace(self, a: np.ndarray, block_size: int) -> np.ndarray:
+        """The reference's Workspace() after Factorize() (compact-only mode),
+        as a dense upper triangle (n x n, zero below the diagonal)."""
+        n = a.shape[0]
+        src = np.ascontiguousarray(a, dtype=np.float64)
+        out = np.zeros((n, n))
+        if self.lib.ref_factor_workspace(n, block_size, _ptr(src), n, _ptr(out), n) != 0:
+            raise RuntimeError("reference factorization threw")
+        return out
 
     def factor_full(self, a: np.ndarray, block_size: int):
         n = a.shape[0]

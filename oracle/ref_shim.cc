@@ -107,6 +107,20 @@ int ref_factor(int n, int b, const double* a, long long lda, double* out,
   }
 }
 
+// Compact-only factorization; `out` (ldo) receives the upper triangle of
+// Workspace() in its final geometry.
+int ref_factor_workspace(int n, int b, const double* a, long long lda, double* out, long long ldo) {
+  try {
+    BlockMatrix input = FillFromDense(n, b, a, lda);
+    BlockLdltDecomposition dec(input, BlockLdltDecomposition::FactorizationMode::kCompactOnly);
+    dec.Factorize();
+    ExtractUpper(dec.Workspace(), out, ldo);
+    return 0;
+  } catch (const std::exception&) {
+    return 1;
+  }
+}
+
 // Full mode: ReconstructOriginal() (n x n row-major) plus LFactor/DFactor.
 int ref_factor_full(int n, int b, const double* a, long long lda,
                     double* reconstructed, double* l_out, double* d_out) {

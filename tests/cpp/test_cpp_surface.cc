@@ -191,9 +191,11 @@ void GeometryFixtures(const std::string& path) {
     for (int& v : geo) in >> v;
     for (int& v : perm) in >> v;
     for (int& v : piv) in >> v;
-    RegularMatrix want(n, n);
+    RegularMatrix want(n, n), want_ws(n, n);
     for (int i = 0; i < n; ++i)
       for (int j = 0; j < n; ++j) in >> want(i, j);
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < n; ++j) in >> want_ws(i, j);
     BlockLdltDecomposition d(BlockMatrix(RandomSymmetric(n, seed), b),
                              BlockLdltDecomposition::FactorizationMode::kCompactOnly);
     d.SetUpdateMode(BBK_UPDATE_FP64_ORDERED);
@@ -212,6 +214,19 @@ void GeometryFixtures(const std::string& path) {
     const RegularMatrix got = f.ToUpperRegular();
     for (int i = 0; i < n; ++i)
       for (int j = 0; j < n; ++j) Require(got(i, j) == want(i, j), "factor bits vs reference");
+    // Workspace(): the reference's workspace rows bit for bit outside the
+    // diagonal blocks, zero inside them
+    const BlockMatrix& w = d.Workspace();
+    for (int bc = 0; bc < w.num_blocks(); ++bc)
+      for (int br = 0; br <= bc; ++br) {
+        const Block& blk = w.GetBlock(br, bc);
+        for (int r = 0; r < blk.rows(); ++r)
+          for (int c = 0; c < blk.cols(); ++c) {
+            const int gi = blk.row0() + r, gj = blk.col0() + c;
+            const double expect = br == bc ? 0.0 : want_ws(gi, gj);
+            Require(blk(r, c) == expect, "workspace rows vs reference");
+          }
+      }
   }
 }
 

@@ -13,8 +13,8 @@ reference's outputs for an input that the tests can regenerate exactly:
 * ``ref_geometry.txt``: cases with several boundary shifts (the reference
   tests' generator, so C++ can regenerate the input): the reference's block
   geometry after factorization (row0, rows, col0, cols per block id), its
-  permutation, pivot types and compact upper factor (%.17g), read by
-  tests/cpp/test_cpp_surface.cc.
+  permutation, pivot types, compact upper factor and the upper triangle of
+  its Workspace() (%.17g), read by tests/cpp/test_cpp_surface.cc.
 
 * ``ref_kkt10000.npz`` (``--kkt``, a few minutes): the saddle-point
   workload at full size (n=10000, H 8000, block 128) from
@@ -154,6 +154,9 @@ def main():
             up = np.triu(r.factors)
             for i in range(n):
                 fh.write(" ".join(f"{x:.17g}" for x in up[i]) + "\n")
+            ws = ref.workspace(a, b)
+            for i in range(n):
+                fh.write(" ".join(f"{x:.17g}" for x in ws[i]) + "\n")
     print(f"wrote {len(names)} small cases, {len(large)} large cases, {len(geo_cases)} geometry cases")
 
 

@@ -192,3 +192,24 @@ def test_bounded_wait_times_out_and_context_survives(cuda, bbk):
     d = bbk.BlockLdltDecomposition(GOLDEN_4x4, 2)
     d.factorize()
     assert d.pivot_types().tolist() == GOLDEN_4x4_PIVOTS
+
+
+@pytest.mark.parametrize("n,b,seed", [(60, 4, 2), (333, 64, 4), (1200, 128, 5)])
+def test_workspace_rows_and_log_bitwise_ordered(cuda, bbk, port, n, b, seed):
+    # bbk_factor_device_ex in the ordered mode: the workspace rows (each
+    # panel's W rows at its trailing columns) bitwise the oracle's, which
+    # tests/test_oracle.py pins to the reference's Workspace(), and the
+    # decision log equal to the oracle's (the same values were compared)
+    import torch
+    a = uniform_symmetric(n, seed)
+    f = torch.from_numpy(a).to(cuda)
+    w = torch.zeros(n, n, dtype=torch.float64, device=cuda)
+    perm, pt, pe, log = bbk.factor_device_logged(f, b, mode="fp64_ordered", workspace_rows=w)
+    want_f, want_log, want_w = port.factor_logged(a, b, workspace_rows=True)
+    assert np.array_equal(w.cpu().numpy(), want_w)
+    got_log = log.cpu().numpy()
+    started = ~np.isnan(got_log[:, 0])
+    assert np.array_equal(started, ~np.isnan(want_log[:, 0]))
+    assert np.array_equal(got_log[started][:, :2], want_log[started][:, :2])
+    assert np.array_equal(np.nan_to_num(got_log[started][:, 2:4], nan=-1.0),
+                          np.nan_to_num(want_log[started][:, 3:5], nan=-1.0))

@@ -138,3 +138,59 @@ def test_oracle_reproduces_the_reference_kkt10000_fixture(port):
     assert np.array_equal(f.perm, z["perm"])
     assert np.array_equal(f.pivot_types, z["pivot_types"].astype(np.int32))
     assert np.array_equal(f.panel_end, z["panel_end"])
+
+
+def test_sampled_residual_restatement(port):
+    # SampledRelativeResidual (tests/block_ldlt_large_stress_test.cc:220-244)
+    # on the reference's own sample set: its first four samples are fixed
+    # (:207-210), and at a size where the full reconstruction fits it agrees
+    # with the residual of those entries of P^T L D L^T P
+    n, b = 300, 32
+    a = uniform_symmetric(n, 77)
+    f = port.factor(a, b)
+    rows, cols = port.residual_samples(n, 3, 4096)
+    assert list(zip(rows[:4], cols[:4])) == [(0, 0), (0, n - 1), (n // 2, n // 2), (n - 1, n - 1)]
+    got = port.sampled_residual(a, f, rows, cols)
+    rec = reconstruct(f.factors, f.perm, f.pivot_types)
+    d = rec[rows, cols] - a[rows, cols]
+    want = np.sqrt(np.sum(d * d)) / max(np.sqrt(np.sum(a[rows, cols] ** 2)), 1.0)
+    assert got < 1e-12
+    assert abs(got - want) <= 0.5 * want + 1e-16
+
+
+@pytest.mark.parametrize("n,b", [(4, 2), (37, 5), (64, 16)])
+def test_reference_full_mode_factors(reference, port, n, b):
+    # the reference's own LFactor()/DFactor() (kFull mode) equal the dense
+    # extraction of the compact factors that the GPU tests use
+    # (ExtractRegularFactorsFromCompact, src/block_ldlt_decomposition.cc:746-763)
+    a = uniform_symmetric(n, 900 + n)
+    rec, lf, df = reference.factor_full(a, b)
+    f = port.factor(a, b)
+    two = np.where(f.pivot_types == 2)[0]
+    lt = np.triu(f.factors, 1)
+    lt[two, two + 1] = 0.0
+    l = lt.T.copy()
+    l[np.diag_indices(n)] = 1.0
+    d = np.diag(np.diag(f.factors))
+    d[two, two + 1] = f.factors[two, two + 1]
+    d[two + 1, two] = f.factors[two, two + 1]
+    assert np.array_equal(lf, l)
+    assert np.array_equal(df, d)
+    assert relative_error(rec, a) < TOLERANCE
+
+
+@pytest.mark.parametrize("n,b,seed", [(40, 7, 1), (60, 4, 2), (200, 32, 3), (333, 64, 4)])
+def test_workspace_rows_match_the_reference(reference, port, n, b, seed):
+    # each panel's W rows at the columns its trailing update reads: exactly
+    # the reference's Workspace() outside the diagonal blocks (the first two
+    # cases include boundary shifts)
+    a = uniform_symmetric(n, seed)
+    f, _, w = port.factor_logged(a, b, workspace_rows=True)
+    ws = reference.workspace(a, b)
+    mask = np.zeros((n, n), bool)
+    k0 = 0
+    for e in f.panel_end:
+        mask[k0:e, e:] = True
+        k0 = e
+    assert np.array_equal(w[mask], ws[mask])
+    assert np.all(w[~mask] == 0.0)
