@@ -883,7 +883,7 @@ def batched_results(args, world: int, rank: int, dev) -> dict:
         return worst
 
     results = {}
-    sampler = ClockSampler(local)
+    sampler = ClockSampler(dev.index if dev.index is not None else 0)
     for mode, refine in (("fp64", False), ("fp32", True)):
         g_step = graph_for(mode, refine)
         g_kern = graph_for(mode, refine, restore=False)

@@ -1027,24 +1027,342 @@ __global__ void __launch_bounds__(kThreadsMma) bf16s_update_kernel(UpdArgs U, co
   cp_async_wait<0>();
 }
 
+// ---------------------------------------------------------------------------
+// BF16 update on the 5th-generation tensor cores (tcgen05 / UMMA).
+//
+// The split operands (split_kernel: kTerms scaled BF16 terms per operand, k
+// contiguous, zero-padded to kpad) are staged by cp.async into shared memory
+// in the no-swizzle K-major core-matrix layout (8 rows x 16 bytes per core
+// matrix; core matrices 128 bytes apart along k, 512 bytes apart along the
+// rows), and one thread issues tcgen05.mma.kind::f16 (M = N = 128, K = 16)
+// for every product t_a(A) t_b(B), a + b < kTerms, smallest first, into one
+// FP32 accumulator in tensor memory (128 lanes x 128 columns).  Completion is
+// tracked by tcgen05.commit on one mbarrier per stage; every wait is bounded
+// and a wait that runs out aborts the factorization with BBK_ERR_TIMEOUT.
+// The epilogue reads the accumulator with tcgen05.ld (warp w: lanes 32w..,
+// one C row per thread), unscales it and subtracts it from the FP64 trailing
+// matrix.  Two CTAs per SM, each with its own accumulator, so one CTA's
+// epilogue (the C traffic, which bounds this kernel) overlaps the other's
+// MMAs.
+// ---------------------------------------------------------------------------
+constexpr int kUM = 128, kUN = 128, kUK = 32;  // C tile, k chunk (BF16 elements)
+constexpr int kUThreads = 128;                  // 4 warps = the accumulator's 128 lanes
+constexpr int kUOpBytes = kUM * kUK * 2;        // one term of one operand per stage
+
+template <int kTerms>
+struct USmem {
+  static constexpr int kStageBytes = 2 * kTerms * kUOpBytes;
+  static constexpr int kStages = kTerms == 3 ? 2 : 4;
+  static constexpr size_t kBytes = static_cast<size_t>(kStages) * kStageBytes + 256;
+};
+static_assert(2 * USmem<3>::kBytes + 2048 <= 228 * 1024, "two CTAs per SM");
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor, SWIZZLE_NONE K-major: start address,
+// leading (k-direction) and stride (row-direction) byte offsets, version 1.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
+  constexpr uint64_t kLbo = 128 >> 4, kSbo = 512 >> 4;
+  return (static_cast<uint64_t>((saddr >> 4) & 0x3FFF)) | (kLbo << 16) | (kSbo << 32) | (1ull << 46);
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulate, BF16 A and B, both
+// K-major, N = 128, M = 128.
+constexpr uint32_t kUIdesc = (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(kUN >> 3) << 17) |
+                             (static_cast<uint32_t>(kUM >> 4) << 24);
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(kUIdesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t mbar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(done)
+      : "r"(mbar), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+// Bounded wait for phase `parity` of mbarrier `mbar`: false when it ran out
+// (or another kernel of the factorization aborted).
+__device__ bool mbar_wait(uint32_t mbar, uint32_t parity, const DeviceState* st, unsigned long long timeout_ns) {
+  unsigned long long t0 = 0;
+  for (unsigned it = 1;; ++it) {
+    if (mbar_try(mbar, parity)) return true;
+    if ((it & 63u) == 0) {
+      const unsigned long long now = globaltimer_ns();
+      if (t0 == 0) t0 = now;
+      if (now - t0 > timeout_ns || ld_relaxed_s32(&st->abort)) return false;
+    }
+  }
+}
+
+template <int kTerms>
+__global__ void __launch_bounds__(kUThreads) umma_bf16s_update_kernel(UpdArgs U, const __nv_bfloat16* ah,
+                                                                      const __nv_bfloat16* bh, int kpad,
+                                                                      size_t term_stride,
+                                                                      unsigned long long timeout_ns) {
+  using S = USmem<kTerms>;
+  extern __shared__ __align__(1024) unsigned char usm[];
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(usm + S::kStages * S::kStageBytes);  // one per stage
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + S::kStages);
+  __shared__ int s_ok;
+  // resolve the panel's range (the split operands start at split_i0, the
+  // 64-aligned row at or below the trailing matrix; tiles here are 128-aligned)
+  if (ld_relaxed_s32(&U.st->abort)) return;
+  const int k0p = ldcg(&U.st->kstart[U.panel & 1]);
+  const int e = ldcg(&U.st->kstart[(U.panel + 1) & 1]);
+  const int inner = e - k0p;
+  if (inner <= 0 || e >= U.n) return;
+  const int split_i0 = (e / kBM) * kBM;
+  const int rows = U.n - split_i0;  // rows of the split operands
+  const int t_i0 = (e / kUM) * kUM;
+  const int tm = (U.n - t_i0 + kUM - 1) / kUM;
+  const int ntiles = tm * (tm + 1) / 2;
+  if (static_cast<int>(blockIdx.x) >= ntiles) return;
+  const int nchunks = (inner + kUK - 1) / kUK;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(kUN)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S::kStages; ++s)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[s])) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_ok = 1;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  auto tile_of = [&](int t, int& i0, int& j0) {
+    int j = static_cast<int>((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+    while (j > 0 && j * (j + 1) / 2 > t) --j;
+    while ((j + 1) * (j + 2) / 2 <= t) ++j;
+    i0 = t_i0 + (t - j * (j + 1) / 2) * kUM;
+    j0 = t_i0 + j * kUN;
+  };
+  // chunk ch of tile (i0, j0) into stage st: per operand and term, 128 rows
+  // x 32 k, row r's k-chunk c (8 elements) at (r/8)*512 + c*128 + (r%8)*16
+  auto load = [&](int st, int i0, int j0, int ch) {
+    unsigned char* base = usm + st * S::kStageBytes;
+    constexpr int kPer = kUM * (kUK / 8);  // 16-byte chunks per operand term
+    for (int q = threadIdx.x; q < 2 * kTerms * kPer; q += kUThreads) {
+      const int blk = q / kPer, rem = q - blk * kPer;  // blk = op * kTerms + term
+      const int r = rem >> 2, c = rem & 3;
+      const int op = blk / kTerms, term = blk - op * kTerms;
+      const int row = (op == 0 ? i0 : j0) - split_i0 + r;
+      const bool ok = row >= 0 && row < rows;
+      const __nv_bfloat16* src = (op == 0 ? ah : bh) + term * term_stride +
+                                 static_cast<size_t>(ok ? row : 0) * kpad + ch * kUK + c * 8;
+      const uint32_t dst = smem_u32(base + blk * kUOpBytes + (r >> 3) * 512 + c * 128 + (r & 7) * 16);
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(ok ? 16 : 0)
+                   : "memory");
+    }
+  };
+  const int my_tiles = (ntiles - static_cast<int>(blockIdx.x) + static_cast<int>(gridDim.x) - 1) /
+                       static_cast<int>(gridDim.x);
+  const long long items = static_cast<long long>(my_tiles) * nchunks;
+  long long ld_item = 0;
+  int ld_ch = 0, ld_m = 0, ld_i0 = 0, ld_j0 = 0;
+  tile_of(blockIdx.x, ld_i0, ld_j0);
+  auto issue = [&]() {
+    if (ld_item < items) {
+      load(static_cast<int>(ld_item % S::kStages), ld_i0, ld_j0, ld_ch);
+      ++ld_item;
+      if (++ld_ch == nchunks) {
+        ld_ch = 0;
+        if (++ld_m < my_tiles) tile_of(static_cast<int>(blockIdx.x) + ld_m * static_cast<int>(gridDim.x), ld_i0, ld_j0);
+      }
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  for (int s = 0; s < S::kStages - 1; ++s) issue();
+
+  bool ok = true;
+  long long item = 0, committed = -1;  // last item whose MMAs were committed
+  for (int m = 0; m < my_tiles && ok; ++m) {
+    int i0, j0;
+    tile_of(static_cast<int>(blockIdx.x) + m * static_cast<int>(gridDim.x), i0, j0);
+    for (int ch = 0; ch < nchunks; ++ch, ++item) {
+      const int st = static_cast<int>(item % S::kStages);
+      asm volatile("cp.async.wait_group %0;" ::"n"(S::kStages - 2) : "memory");
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // copies visible to the tensor core
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncthreads();
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      if (threadIdx.x == 0) {
+        const uint32_t sb = smem_u32(usm + st * S::kStageBytes);
+        for (int ia = kTerms - 1; ia >= 0; --ia)
+          for (int ib = kTerms - 1 - ia; ib >= 0; --ib) {
+            const uint32_t a0 = sb + ia * kUOpBytes, b0 = sb + (kTerms + ib) * kUOpBytes;
+#pragma unroll
+            for (int ks = 0; ks < kUK / 16; ++ks) {
+              const bool first = ch == 0 && ks == 0 && ia == kTerms - 1 && ib == kTerms - 1 - ia;
+              umma_bf16(tmem, umma_desc(a0 + ks * 256), umma_desc(b0 + ks * 256), first ? 0u : 1u);
+            }
+          }
+        umma_commit(smem_u32(&mbar[st]));
+      }
+      committed = item;
+      // the stage refilled next held item - 1: wait until its MMAs are done
+      if (item >= 1) {
+        const long long prev = item - 1;
+        if (!mbar_wait(smem_u32(&mbar[prev % S::kStages]), static_cast<uint32_t>((prev / S::kStages) & 1),
+                       U.st, timeout_ns))
+          ok = false;
+      }
+      if (!__syncthreads_and(ok)) {
+        ok = false;
+        break;
+      }
+      issue();
+    }
+    if (!ok) break;
+    // the tile's last MMAs: wait, then read the accumulator
+    const long long last = item - 1;
+    ok = mbar_wait(smem_u32(&mbar[last % S::kStages]), static_cast<uint32_t>((last / S::kStages) & 1), U.st,
+                   timeout_ns);
+    if (!__syncthreads_and(ok)) {
+      ok = false;
+      break;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const int i = i0 + warp * 32 + lane;  // this thread's row of the tile
+    const bool row_ok = i >= e && i < U.n;
+    const int is = min(max(i, split_i0), U.n - 1);  // scale block of a row inside the matrix
+    const double sa = U.a_scale[(is - split_i0) / kBM];
+    double* crow = U.c + static_cast<long long>(is) * U.ldc;
+#pragma unroll 1
+    for (int c0 = 0; c0 < kUN; c0 += 16) {
+      uint32_t v[16];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+          "%14, %15}, [%16];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+          : "r"(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c0)));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      const int jb = j0 + c0;
+      const int js = min(max(jb, split_i0), U.n - 1);
+      const double unscale = 1.0 / (sa * U.b_scale[(js - split_i0) / kBM]);
+      if (row_ok) {
+#pragma unroll
+        for (int u = 0; u < 16; u += 2) {
+          const int j = jb + u;
+          const double v0 = static_cast<double>(__uint_as_float(v[u])) * unscale;
+          const double v1 = static_cast<double>(__uint_as_float(v[u + 1])) * unscale;
+          const bool ok0 = j >= e && j < U.n && i <= j;
+          const bool ok1 = j + 1 >= e && j + 1 < U.n && i <= j + 1;
+          if (ok0 && ok1) {
+            double2 cv = *reinterpret_cast<const double2*>(crow + j);
+            cv.x -= v0;
+            cv.y -= v1;
+            *reinterpret_cast<double2*>(crow + j) = cv;
+          } else {
+            if (ok0) crow[j] -= v0;
+            if (ok1) crow[j + 1] -= v1;
+          }
+        }
+      }
+    }
+    // every warp has read the accumulator before the next tile overwrites it
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+  }
+  asm volatile("cp.async.wait_all;" ::: "memory");
+  if (!ok && threadIdx.x == 0) {
+    atomicCAS(const_cast<int*>(&U.st->status), 0, BBK_ERR_TIMEOUT);
+    atomicExch(const_cast<int*>(&U.st->abort), 1);
+    // let MMAs already issued finish before the accumulator is released (a
+    // bounded wait; the abort flag is set, so use a plain time bound)
+    if (committed >= 0) {
+      const uint32_t mb = smem_u32(&mbar[committed % S::kStages]);
+      const uint32_t par = static_cast<uint32_t>((committed / S::kStages) & 1);
+      const unsigned long long t0 = globaltimer_ns();
+      while (!mbar_try(mb, par) && globaltimer_ns() - t0 < timeout_ns) {
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kUN) : "memory");
+}
+
+template <int kTerms>
+int launch_umma_bf16(const UpdArgs& U, const __nv_bfloat16* ah, const __nv_bfloat16* bh, int kpad,
+                     size_t term_stride, long long order, cudaStream_t s) {
+  using S = USmem<kTerms>;
+  static std::once_flag attr_once[64];
+  int dev = 0;
+  BBK_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return set_error(BBK_ERR_NO_DEVICE, "device %d out of range", dev);
+  cudaError_t attr_err = cudaSuccess;
+  std::call_once(attr_once[dev], [&] {
+    attr_err = cudaFuncSetAttribute(umma_bf16s_update_kernel<kTerms>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(S::kBytes));
+  });
+  BBK_CUDA_TRY(attr_err);
+  const long long tm = (order + kUM - 1) / kUM + 1;
+  const long long tiles = tm * (tm + 1) / 2;
+  const int grid = static_cast<int>(std::max(1LL, std::min<long long>(tiles, 2LL * device_sm_count())));
+  umma_bf16s_update_kernel<kTerms><<<grid, kUThreads, S::kBytes, s>>>(U, ah, bh, kpad, term_stride,
+                                                                      wait_timeout_ns());
+  BBK_CUDA_TRY(cudaGetLastError());
+  count_launch();
+  return BBK_OK;
+}
+
+// BF16 updates on tcgen05 (default) or the warp-level MMA kernel
+// (BBK_BF16_UMMA=0: comparison).
+bool use_umma_bf16() {
+  static const bool v = [] {
+    const char* e = getenv("BBK_BF16_UMMA");
+    return e ? atoi(e) != 0 : true;
+  }();
+  return v;
+}
+
 template <int kTerms>
 int launch_bf16_split(const UpdArgs& U, __nv_bfloat16* buf, int kpad, size_t term_stride, int grid_mma, bool vec,
-                      cudaStream_t s) {
+                      long long order, cudaStream_t s) {
   const int sms = device_sm_count();
   __nv_bfloat16* ah = buf;
   __nv_bfloat16* bh = buf + static_cast<size_t>(kTerms) * term_stride;
   split_kernel<kTerms><<<4 * sms, 256, 0, s>>>(U, ah, bh, kpad, term_stride);
   BBK_CUDA_TRY(cudaGetLastError());
   count_launch();
+  if (vec && use_umma_bf16()) return launch_umma_bf16<kTerms>(U, ah, bh, kpad, term_stride, order, s);
   const size_t bytes = HSmem<kTerms>::kBytes;
-  static bool attr_set[64] = {};
+  static std::once_flag attr_once[64];
   int dev = 0;
   BBK_CUDA_TRY(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 64 || !attr_set[dev]) {
-    BBK_CUDA_TRY(cudaFuncSetAttribute(bf16s_update_kernel<kTerms>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      static_cast<int>(bytes)));
-    if (dev >= 0 && dev < 64) attr_set[dev] = true;
-  }
+  if (dev < 0 || dev >= 64) return set_error(BBK_ERR_NO_DEVICE, "device %d out of range", dev);
+  cudaError_t attr_err = cudaSuccess;
+  std::call_once(attr_once[dev], [&] {
+    attr_err = cudaFuncSetAttribute(bf16s_update_kernel<kTerms>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(bytes));
+  });
+  BBK_CUDA_TRY(attr_err);
   bf16s_update_kernel<kTerms><<<grid_mma, kThreadsMma, bytes, s>>>(U, ah, bh, kpad, term_stride, vec ? 1 : 0);
   BBK_CUDA_TRY(cudaGetLastError());
   count_launch();
@@ -1189,8 +1507,8 @@ int launch_update(const FactorPlan& plan, int panel, cudaStream_t s) {
     count_launch();
     auto* buf = static_cast<__nv_bfloat16*>(plan.hsplit);
     return plan.mode == BBK_UPDATE_BF16
-               ? launch_bf16_split<1>(U, buf, plan.kpad, plan.hstride, grid_mma, vec, s)
-               : launch_bf16_split<3>(U, buf, plan.kpad, plan.hstride, grid_mma, vec, s);
+               ? launch_bf16_split<1>(U, buf, plan.kpad, plan.hstride, grid_mma, vec, plan.n - nominal_e, s)
+               : launch_bf16_split<3>(U, buf, plan.kpad, plan.hstride, grid_mma, vec, plan.n - nominal_e, s);
   }
   if (plan.mode == BBK_UPDATE_FP64 && vec) {
     bool launched = false;
