@@ -1045,14 +1045,19 @@ __global__ void __launch_bounds__(kThreadsMma) bf16s_update_kernel(UpdArgs U, co
 // epilogue (the C traffic, which bounds this kernel) overlaps the other's
 // MMAs.
 // ---------------------------------------------------------------------------
-constexpr int kUM = 128, kUN = 128, kUK = 32;  // C tile, k chunk (BF16 elements)
-constexpr int kUThreads = 128;                  // 4 warps = the accumulator's 128 lanes
-constexpr int kUOpBytes = kUM * kUK * 2;        // one term of one operand per stage
+constexpr int kUM = 128, kUN = 128;  // C tile
+constexpr int kUThreads = 128;        // 4 warps = the accumulator's 128 lanes
 
+// Per term count: the k chunk (BF16 elements) and the stages, sized so that
+// two CTAs fit one SM with the same bytes in flight (three terms: more,
+// shorter stages, so a stage is refilled soon after its MMAs finish).
 template <int kTerms>
 struct USmem {
-  static constexpr int kStageBytes = 2 * kTerms * kUOpBytes;
-  static constexpr int kStages = kTerms == 3 ? 2 : 4;
+  static constexpr int kK = kTerms == 3 ? 16 : 32;
+  static constexpr int kOpBytes = kUM * kK * 2;  // one term of one operand per stage
+  static constexpr int kRowGroup = (kK / 8) * 128;  // bytes between 8-row core-matrix groups
+  static constexpr int kStageBytes = 2 * kTerms * kOpBytes;
+  static constexpr int kStages = 4;
   static constexpr size_t kBytes = static_cast<size_t>(kStages) * kStageBytes + 256;
 };
 static_assert(2 * USmem<3>::kBytes + 2048 <= 228 * 1024, "two CTAs per SM");
@@ -1062,10 +1067,12 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
 }
 
 // Shared-memory matrix descriptor, SWIZZLE_NONE K-major: start address,
-// leading (k-direction) and stride (row-direction) byte offsets, version 1.
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
-  constexpr uint64_t kLbo = 128 >> 4, kSbo = 512 >> 4;
-  return (static_cast<uint64_t>((saddr >> 4) & 0x3FFF)) | (kLbo << 16) | (kSbo << 32) | (1ull << 46);
+// leading (k-direction, 128 B) and stride (row-direction) byte offsets,
+// version 1.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t sbo) {
+  constexpr uint64_t kLbo = 128 >> 4;
+  return (static_cast<uint64_t>((saddr >> 4) & 0x3FFF)) | (kLbo << 16) |
+         (static_cast<uint64_t>(sbo >> 4) << 32) | (1ull << 46);
 }
 
 // Instruction descriptor of kind::f16: FP32 accumulate, BF16 A and B, both
@@ -1132,6 +1139,8 @@ __global__ void __launch_bounds__(kUThreads) umma_bf16s_update_kernel(UpdArgs U,
   const int tm = (U.n - t_i0 + kUM - 1) / kUM;
   const int ntiles = tm * (tm + 1) / 2;
   if (static_cast<int>(blockIdx.x) >= ntiles) return;
+  constexpr int kUK = S::kK;
+  constexpr int kUOpBytes = S::kOpBytes;
   const int nchunks = (inner + kUK - 1) / kUK;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
@@ -1160,19 +1169,21 @@ __global__ void __launch_bounds__(kUThreads) umma_bf16s_update_kernel(UpdArgs U,
     j0 = t_i0 + j * kUN;
   };
   // chunk ch of tile (i0, j0) into stage st: per operand and term, 128 rows
-  // x 32 k, row r's k-chunk c (8 elements) at (r/8)*512 + c*128 + (r%8)*16
+  // x kUK k, row r's k-chunk c (8 elements) at (r/8)*kRowGroup + c*128 +
+  // (r%8)*16
   auto load = [&](int st, int i0, int j0, int ch) {
     unsigned char* base = usm + st * S::kStageBytes;
-    constexpr int kPer = kUM * (kUK / 8);  // 16-byte chunks per operand term
+    constexpr int kCols = kUK / 8;         // 16-byte chunks per row
+    constexpr int kPer = kUM * kCols;      // 16-byte chunks per operand term
     for (int q = threadIdx.x; q < 2 * kTerms * kPer; q += kUThreads) {
       const int blk = q / kPer, rem = q - blk * kPer;  // blk = op * kTerms + term
-      const int r = rem >> 2, c = rem & 3;
+      const int r = rem / kCols, c = rem % kCols;
       const int op = blk / kTerms, term = blk - op * kTerms;
       const int row = (op == 0 ? i0 : j0) - split_i0 + r;
       const bool ok = row >= 0 && row < rows;
       const __nv_bfloat16* src = (op == 0 ? ah : bh) + term * term_stride +
                                  static_cast<size_t>(ok ? row : 0) * kpad + ch * kUK + c * 8;
-      const uint32_t dst = smem_u32(base + blk * kUOpBytes + (r >> 3) * 512 + c * 128 + (r & 7) * 16);
+      const uint32_t dst = smem_u32(base + blk * kUOpBytes + (r >> 3) * S::kRowGroup + c * 128 + (r & 7) * 16);
       asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(ok ? 16 : 0)
                    : "memory");
     }
@@ -1201,6 +1212,15 @@ __global__ void __launch_bounds__(kUThreads) umma_bf16s_update_kernel(UpdArgs U,
   for (int m = 0; m < my_tiles && ok; ++m) {
     int i0, j0;
     tile_of(static_cast<int>(blockIdx.x) + m * static_cast<int>(gridDim.x), i0, j0);
+    {
+      // this thread's C row of the tile goes to L2 while the MMAs run
+      const int i = i0 + threadIdx.x;
+      if (i >= e && i < U.n) {
+        const double* row = U.c + static_cast<long long>(i) * U.ldc;
+        for (int jc = max(j0, i) & ~15; jc < min(j0 + kUN, U.n); jc += 16)
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(row + jc));
+      }
+    }
     for (int ch = 0; ch < nchunks; ++ch, ++item) {
       const int st = static_cast<int>(item % S::kStages);
       asm volatile("cp.async.wait_group %0;" ::"n"(S::kStages - 2) : "memory");
@@ -1216,7 +1236,8 @@ __global__ void __launch_bounds__(kUThreads) umma_bf16s_update_kernel(UpdArgs U,
 #pragma unroll
             for (int ks = 0; ks < kUK / 16; ++ks) {
               const bool first = ch == 0 && ks == 0 && ia == kTerms - 1 && ib == kTerms - 1 - ia;
-              umma_bf16(tmem, umma_desc(a0 + ks * 256), umma_desc(b0 + ks * 256), first ? 0u : 1u);
+              umma_bf16(tmem, umma_desc(a0 + ks * 256, S::kRowGroup), umma_desc(b0 + ks * 256, S::kRowGroup),
+                        first ? 0u : 1u);
             }
           }
         umma_commit(smem_u32(&mbar[st]));
@@ -1250,6 +1271,27 @@ __global__ void __launch_bounds__(kUThreads) umma_bf16s_update_kernel(UpdArgs U,
     const int is = min(max(i, split_i0), U.n - 1);  // scale block of a row inside the matrix
     const double sa = U.a_scale[(is - split_i0) / kBM];
     double* crow = U.c + static_cast<long long>(is) * U.ldc;
+    // C values of the 16-column group at c0 (entries this thread does not
+    // update read as 0); the next group's load is in flight while a group
+    // is updated
+    auto load_c = [&](int c0, double (&cv)[16]) {
+#pragma unroll
+      for (int u = 0; u < 16; u += 2) {
+        const int j = j0 + c0 + u;
+        const bool ok0 = row_ok && j >= e && j < U.n && i <= j;
+        const bool ok1 = row_ok && j + 1 >= e && j + 1 < U.n && i <= j + 1;
+        if (ok0 && ok1) {
+          const double2 t = *reinterpret_cast<const double2*>(crow + j);
+          cv[u] = t.x;
+          cv[u + 1] = t.y;
+        } else {
+          cv[u] = ok0 ? crow[j] : 0.0;
+          cv[u + 1] = ok1 ? crow[j + 1] : 0.0;
+        }
+      }
+    };
+    double cur[16], nxt[16];
+    load_c(0, cur);
 #pragma unroll 1
     for (int c0 = 0; c0 < kUN; c0 += 16) {
       uint32_t v[16];
@@ -1259,6 +1301,7 @@ __global__ void __launch_bounds__(kUThreads) umma_bf16s_update_kernel(UpdArgs U,
           : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
             "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
           : "r"(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c0)));
+      if (c0 + 16 < kUN) load_c(c0 + 16, nxt);
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
       const int jb = j0 + c0;
       const int js = min(max(jb, split_i0), U.n - 1);
@@ -1267,21 +1310,20 @@ __global__ void __launch_bounds__(kUThreads) umma_bf16s_update_kernel(UpdArgs U,
 #pragma unroll
         for (int u = 0; u < 16; u += 2) {
           const int j = jb + u;
-          const double v0 = static_cast<double>(__uint_as_float(v[u])) * unscale;
-          const double v1 = static_cast<double>(__uint_as_float(v[u + 1])) * unscale;
+          const double v0 = cur[u] - static_cast<double>(__uint_as_float(v[u])) * unscale;
+          const double v1 = cur[u + 1] - static_cast<double>(__uint_as_float(v[u + 1])) * unscale;
           const bool ok0 = j >= e && j < U.n && i <= j;
           const bool ok1 = j + 1 >= e && j + 1 < U.n && i <= j + 1;
           if (ok0 && ok1) {
-            double2 cv = *reinterpret_cast<const double2*>(crow + j);
-            cv.x -= v0;
-            cv.y -= v1;
-            *reinterpret_cast<double2*>(crow + j) = cv;
+            *reinterpret_cast<double2*>(crow + j) = make_double2(v0, v1);
           } else {
-            if (ok0) crow[j] -= v0;
-            if (ok1) crow[j + 1] -= v1;
+            if (ok0) crow[j] = v0;
+            if (ok1) crow[j + 1] = v1;
           }
         }
       }
+#pragma unroll
+      for (int u = 0; u < 16; ++u) cur[u] = nxt[u];
     }
     // every warp has read the accumulator before the next tile overwrites it
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
