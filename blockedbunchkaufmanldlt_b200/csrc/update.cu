@@ -1058,7 +1058,9 @@ struct USmem {
   static constexpr int kRowGroup = (kK / 8) * 128;  // bytes between 8-row core-matrix groups
   static constexpr int kStageBytes = 2 * kTerms * kOpBytes;
   static constexpr int kStages = 4;
+  // stages, then the barriers (2 x kStages + 4) and the accumulator address
   static constexpr size_t kBytes = static_cast<size_t>(kStages) * kStageBytes + 256;
+  static_assert((2 * kStages + 4) * 8 + 4 <= 256, "barrier area");
 };
 static_assert(2 * USmem<3>::kBytes + 2048 <= 228 * 1024, "two CTAs per SM");
 
@@ -1116,45 +1118,75 @@ __device__ bool mbar_wait(uint32_t mbar, uint32_t parity, const DeviceState* st,
   }
 }
 
+// Roles (warp-specialized, no CTA barrier inside the main loop):
+//   warps 0-3   epilogue: wait until an accumulator is full, read it with
+//               tcgen05.ld (warp w: lanes 32w..32w+31, one C row per
+//               thread), C -= unscale * acc, then mark the accumulator empty;
+//   warps 4-7   producers: cp.async the next chunk into a free stage and
+//               arrive on that stage's "full" barrier when the copies land;
+//   warp 8      lane 0 issues the MMAs of each full stage, commits them to
+//               the stage's "empty" barrier and, after a tile's last chunk,
+//               to the accumulator's "full" barrier.
+// Two accumulators (2 x 128 TMEM columns) let the epilogue of one tile run
+// while the next tile's MMAs execute.
+constexpr int kUEpi = 4, kUProd = 4;
+constexpr int kUWarps = kUEpi + kUProd + 1;
+constexpr int kUBlock = kUWarps * 32;
+
+__device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mbar) : "memory");
+}
+
 template <int kTerms>
-__global__ void __launch_bounds__(kUThreads) umma_bf16s_update_kernel(UpdArgs U, const __nv_bfloat16* ah,
-                                                                      const __nv_bfloat16* bh, int kpad,
-                                                                      size_t term_stride,
-                                                                      unsigned long long timeout_ns) {
+__global__ void __launch_bounds__(kUBlock, 2) umma_bf16s_update_kernel(UpdArgs U, const __nv_bfloat16* ah,
+                                                                       const __nv_bfloat16* bh, int kpad,
+                                                                       size_t term_stride,
+                                                                       unsigned long long timeout_ns) {
   using S = USmem<kTerms>;
+  constexpr int kUK = S::kK;
+  constexpr int kUOpBytes = S::kOpBytes;
   extern __shared__ __align__(1024) unsigned char usm[];
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(usm + S::kStages * S::kStageBytes);  // one per stage
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + S::kStages);
-  __shared__ int s_ok;
-  // resolve the panel's range (the split operands start at split_i0, the
-  // 64-aligned row at or below the trailing matrix; tiles here are 128-aligned)
+  uint64_t* full = reinterpret_cast<uint64_t*>(usm + S::kStages * S::kStageBytes);
+  uint64_t* empty = full + S::kStages;
+  uint64_t* accfull = empty + S::kStages;  // 2
+  uint64_t* accempty = accfull + 2;        // 2
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accempty + 2);
+  // the panel's range (the split operands start at split_i0, the 64-aligned
+  // row at or below the trailing matrix; tiles here are 128-aligned)
   if (ld_relaxed_s32(&U.st->abort)) return;
   const int k0p = ldcg(&U.st->kstart[U.panel & 1]);
   const int e = ldcg(&U.st->kstart[(U.panel + 1) & 1]);
   const int inner = e - k0p;
   if (inner <= 0 || e >= U.n) return;
   const int split_i0 = (e / kBM) * kBM;
-  const int rows = U.n - split_i0;  // rows of the split operands
+  const int rows = U.n - split_i0;
   const int t_i0 = (e / kUM) * kUM;
   const int tm = (U.n - t_i0 + kUM - 1) / kUM;
   const int ntiles = tm * (tm + 1) / 2;
   if (static_cast<int>(blockIdx.x) >= ntiles) return;
-  constexpr int kUK = S::kK;
-  constexpr int kUOpBytes = S::kOpBytes;
   const int nchunks = (inner + kUK - 1) / kUK;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int my_tiles = (ntiles - static_cast<int>(blockIdx.x) + static_cast<int>(gridDim.x) - 1) /
+                       static_cast<int>(gridDim.x);
 
-  if (warp == 0) {
+  if (warp == kUWarps - 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(kUN)
+                 "r"(2 * kUN)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-  }
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < S::kStages; ++s)
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[s])) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    s_ok = 1;
+    if (lane == 0) {
+      for (int st = 0; st < S::kStages; ++st) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&full[st])), "r"(kUProd * 32)
+                     : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&empty[st])) : "memory");
+      }
+      for (int b = 0; b < 2; ++b) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&accfull[b])) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&accempty[b])), "r"(kUEpi)
+                     : "memory");
+      }
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
@@ -1168,186 +1200,184 @@ __global__ void __launch_bounds__(kUThreads) umma_bf16s_update_kernel(UpdArgs U,
     i0 = t_i0 + (t - j * (j + 1) / 2) * kUM;
     j0 = t_i0 + j * kUN;
   };
-  // chunk ch of tile (i0, j0) into stage st: per operand and term, 128 rows
-  // x kUK k, row r's k-chunk c (8 elements) at (r/8)*kRowGroup + c*128 +
-  // (r%8)*16
-  auto load = [&](int st, int i0, int j0, int ch) {
-    unsigned char* base = usm + st * S::kStageBytes;
-    constexpr int kCols = kUK / 8;         // 16-byte chunks per row
-    constexpr int kPer = kUM * kCols;      // 16-byte chunks per operand term
-    for (int q = threadIdx.x; q < 2 * kTerms * kPer; q += kUThreads) {
-      const int blk = q / kPer, rem = q - blk * kPer;  // blk = op * kTerms + term
-      const int r = rem / kCols, c = rem % kCols;
-      const int op = blk / kTerms, term = blk - op * kTerms;
-      const int row = (op == 0 ? i0 : j0) - split_i0 + r;
-      const bool ok = row >= 0 && row < rows;
-      const __nv_bfloat16* src = (op == 0 ? ah : bh) + term * term_stride +
-                                 static_cast<size_t>(ok ? row : 0) * kpad + ch * kUK + c * 8;
-      const uint32_t dst = smem_u32(base + blk * kUOpBytes + (r >> 3) * S::kRowGroup + c * 128 + (r & 7) * 16);
-      asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(ok ? 16 : 0)
-                   : "memory");
-    }
-  };
-  const int my_tiles = (ntiles - static_cast<int>(blockIdx.x) + static_cast<int>(gridDim.x) - 1) /
-                       static_cast<int>(gridDim.x);
-  const long long items = static_cast<long long>(my_tiles) * nchunks;
-  long long ld_item = 0;
-  int ld_ch = 0, ld_m = 0, ld_i0 = 0, ld_j0 = 0;
-  tile_of(blockIdx.x, ld_i0, ld_j0);
-  auto issue = [&]() {
-    if (ld_item < items) {
-      load(static_cast<int>(ld_item % S::kStages), ld_i0, ld_j0, ld_ch);
-      ++ld_item;
-      if (++ld_ch == nchunks) {
-        ld_ch = 0;
-        if (++ld_m < my_tiles) tile_of(static_cast<int>(blockIdx.x) + ld_m * static_cast<int>(gridDim.x), ld_i0, ld_j0);
+  bool ok = true;
+
+  if (warp >= kUEpi && warp < kUEpi + kUProd) {
+    // ---- producers
+    const int pt = threadIdx.x - kUEpi * 32;
+    constexpr int kCols = kUK / 8;     // 16-byte chunks per row
+    constexpr int kPer = kUM * kCols;  // 16-byte chunks per operand term
+    long long item = 0;
+    for (int m = 0; m < my_tiles && ok; ++m) {
+      int i0, j0;
+      tile_of(static_cast<int>(blockIdx.x) + m * static_cast<int>(gridDim.x), i0, j0);
+      for (int ch = 0; ch < nchunks; ++ch, ++item) {
+        const int st = static_cast<int>(item % S::kStages);
+        const long long use = item / S::kStages;
+        if (use >= 1 && !mbar_wait(smem_u32(&empty[st]), static_cast<uint32_t>((use - 1) & 1), U.st, timeout_ns)) {
+          ok = false;
+          break;
+        }
+        unsigned char* base = usm + st * S::kStageBytes;
+        // per operand and term, 128 rows x kUK k: row r's k-chunk c (8
+        // elements) at (r/8)*kRowGroup + c*128 + (r%8)*16
+        for (int q = pt; q < 2 * kTerms * kPer; q += kUProd * 32) {
+          const int blk = q / kPer, rem = q - blk * kPer;  // blk = op * kTerms + term
+          const int r = rem / kCols, c = rem % kCols;
+          const int op = blk / kTerms, term = blk - op * kTerms;
+          const int row = (op == 0 ? i0 : j0) - split_i0 + r;
+          const bool in = row >= 0 && row < rows;
+          const __nv_bfloat16* src = (op == 0 ? ah : bh) + term * term_stride +
+                                     static_cast<size_t>(in ? row : 0) * kpad + ch * kUK + c * 8;
+          const uint32_t dst =
+              smem_u32(base + blk * kUOpBytes + (r >> 3) * S::kRowGroup + c * 128 + (r & 7) * 16);
+          asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(in ? 16 : 0)
+                       : "memory");
+        }
+        asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(&full[st]))
+                     : "memory");
       }
     }
-    asm volatile("cp.async.commit_group;" ::: "memory");
-  };
-  for (int s = 0; s < S::kStages - 1; ++s) issue();
-
-  bool ok = true;
-  long long item = 0, committed = -1;  // last item whose MMAs were committed
-  for (int m = 0; m < my_tiles && ok; ++m) {
-    int i0, j0;
-    tile_of(static_cast<int>(blockIdx.x) + m * static_cast<int>(gridDim.x), i0, j0);
-    {
-      // this thread's C row of the tile goes to L2 while the MMAs run
-      const int i = i0 + threadIdx.x;
-      if (i >= e && i < U.n) {
+    asm volatile("cp.async.wait_all;" ::: "memory");
+  } else if (warp == kUWarps - 1) {
+    // ---- MMA issue (one thread)
+    if (lane == 0) {
+      long long item = 0;
+      long long committed = -1;  // last stage commit
+      int acc_commits = 0;       // accumulator commits issued
+      for (int m = 0; m < my_tiles && ok; ++m) {
+        const int b = m & 1, v = m >> 1;
+        if (v >= 1 && !mbar_wait(smem_u32(&accempty[b]), static_cast<uint32_t>((v - 1) & 1), U.st, timeout_ns)) {
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t acc = tmem + static_cast<uint32_t>(b * kUN);
+        for (int ch = 0; ch < nchunks; ++ch, ++item) {
+          const int st = static_cast<int>(item % S::kStages);
+          if (!mbar_wait(smem_u32(&full[st]), static_cast<uint32_t>((item / S::kStages) & 1), U.st, timeout_ns)) {
+            ok = false;
+            break;
+          }
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // the copies, to the tensor core
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t sb = smem_u32(usm + st * S::kStageBytes);
+          for (int ia = kTerms - 1; ia >= 0; --ia)
+            for (int ib = kTerms - 1 - ia; ib >= 0; --ib) {
+              const uint32_t a0 = sb + ia * kUOpBytes, b0 = sb + (kTerms + ib) * kUOpBytes;
+#pragma unroll
+              for (int ks = 0; ks < kUK / 16; ++ks) {
+                const bool first = ch == 0 && ks == 0 && ia == kTerms - 1 && ib == kTerms - 1 - ia;
+                umma_bf16(acc, umma_desc(a0 + ks * 256, S::kRowGroup), umma_desc(b0 + ks * 256, S::kRowGroup),
+                          first ? 0u : 1u);
+              }
+            }
+          umma_commit(smem_u32(&empty[st]));
+          committed = item;
+        }
+        if (!ok) break;
+        umma_commit(smem_u32(&accfull[b]));
+        ++acc_commits;
+      }
+      if (!ok && committed >= 0) {
+        // let the MMAs already issued finish before the accumulators are released
+        const uint32_t mb = smem_u32(&empty[committed % S::kStages]);
+        const uint32_t par = static_cast<uint32_t>((committed / S::kStages) & 1);
+        const unsigned long long t0 = globaltimer_ns();
+        while (!mbar_try(mb, par) && globaltimer_ns() - t0 < timeout_ns) {
+        }
+      }
+      (void)acc_commits;
+    }
+  } else {
+    // ---- epilogue
+    for (int m = 0; m < my_tiles && ok; ++m) {
+      const int b = m & 1, v = m >> 1;
+      int i0, j0;
+      tile_of(static_cast<int>(blockIdx.x) + m * static_cast<int>(gridDim.x), i0, j0);
+      const int i = i0 + warp * 32 + lane;  // this thread's row of the tile
+      const bool row_ok = i >= e && i < U.n;
+      if (row_ok) {
         const double* row = U.c + static_cast<long long>(i) * U.ldc;
         for (int jc = max(j0, i) & ~15; jc < min(j0 + kUN, U.n); jc += 16)
           asm volatile("prefetch.global.L2 [%0];" ::"l"(row + jc));
       }
-    }
-    for (int ch = 0; ch < nchunks; ++ch, ++item) {
-      const int st = static_cast<int>(item % S::kStages);
-      asm volatile("cp.async.wait_group %0;" ::"n"(S::kStages - 2) : "memory");
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // copies visible to the tensor core
-      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-      __syncthreads();
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      if (threadIdx.x == 0) {
-        const uint32_t sb = smem_u32(usm + st * S::kStageBytes);
-        for (int ia = kTerms - 1; ia >= 0; --ia)
-          for (int ib = kTerms - 1 - ia; ib >= 0; --ib) {
-            const uint32_t a0 = sb + ia * kUOpBytes, b0 = sb + (kTerms + ib) * kUOpBytes;
-#pragma unroll
-            for (int ks = 0; ks < kUK / 16; ++ks) {
-              const bool first = ch == 0 && ks == 0 && ia == kTerms - 1 && ib == kTerms - 1 - ia;
-              umma_bf16(tmem, umma_desc(a0 + ks * 256, S::kRowGroup), umma_desc(b0 + ks * 256, S::kRowGroup),
-                        first ? 0u : 1u);
-            }
-          }
-        umma_commit(smem_u32(&mbar[st]));
-      }
-      committed = item;
-      // the stage refilled next held item - 1: wait until its MMAs are done
-      if (item >= 1) {
-        const long long prev = item - 1;
-        if (!mbar_wait(smem_u32(&mbar[prev % S::kStages]), static_cast<uint32_t>((prev / S::kStages) & 1),
-                       U.st, timeout_ns))
-          ok = false;
-      }
-      if (!__syncthreads_and(ok)) {
+      if (!mbar_wait(smem_u32(&accfull[b]), static_cast<uint32_t>(v & 1), U.st, timeout_ns)) {
         ok = false;
         break;
       }
-      issue();
-    }
-    if (!ok) break;
-    // the tile's last MMAs: wait, then read the accumulator
-    const long long last = item - 1;
-    ok = mbar_wait(smem_u32(&mbar[last % S::kStages]), static_cast<uint32_t>((last / S::kStages) & 1), U.st,
-                   timeout_ns);
-    if (!__syncthreads_and(ok)) {
-      ok = false;
-      break;
-    }
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const int i = i0 + warp * 32 + lane;  // this thread's row of the tile
-    const bool row_ok = i >= e && i < U.n;
-    const int is = min(max(i, split_i0), U.n - 1);  // scale block of a row inside the matrix
-    const double sa = U.a_scale[(is - split_i0) / kBM];
-    double* crow = U.c + static_cast<long long>(is) * U.ldc;
-    // C values of the 16-column group at c0 (entries this thread does not
-    // update read as 0); the next group's load is in flight while a group
-    // is updated
-    auto load_c = [&](int c0, double (&cv)[16]) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int is = min(max(i, split_i0), U.n - 1);  // scale block of a row inside the matrix
+      const double sa = U.a_scale[(is - split_i0) / kBM];
+      double* crow = U.c + static_cast<long long>(is) * U.ldc;
+      // C values of the 8-column group at c0 (entries this thread does not
+      // update read as 0); the next group's load is in flight while a group
+      // is updated
+      auto load_c = [&](int c0, double (&cv)[8]) {
 #pragma unroll
-      for (int u = 0; u < 16; u += 2) {
-        const int j = j0 + c0 + u;
-        const bool ok0 = row_ok && j >= e && j < U.n && i <= j;
-        const bool ok1 = row_ok && j + 1 >= e && j + 1 < U.n && i <= j + 1;
-        if (ok0 && ok1) {
-          const double2 t = *reinterpret_cast<const double2*>(crow + j);
-          cv[u] = t.x;
-          cv[u + 1] = t.y;
-        } else {
-          cv[u] = ok0 ? crow[j] : 0.0;
-          cv[u + 1] = ok1 ? crow[j + 1] : 0.0;
-        }
-      }
-    };
-    double cur[16], nxt[16];
-    load_c(0, cur);
-#pragma unroll 1
-    for (int c0 = 0; c0 < kUN; c0 += 16) {
-      uint32_t v[16];
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
-          "%14, %15}, [%16];"
-          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-          : "r"(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c0)));
-      if (c0 + 16 < kUN) load_c(c0 + 16, nxt);
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      const int jb = j0 + c0;
-      const int js = min(max(jb, split_i0), U.n - 1);
-      const double unscale = 1.0 / (sa * U.b_scale[(js - split_i0) / kBM]);
-      if (row_ok) {
-#pragma unroll
-        for (int u = 0; u < 16; u += 2) {
-          const int j = jb + u;
-          const double v0 = cur[u] - static_cast<double>(__uint_as_float(v[u])) * unscale;
-          const double v1 = cur[u + 1] - static_cast<double>(__uint_as_float(v[u + 1])) * unscale;
-          const bool ok0 = j >= e && j < U.n && i <= j;
-          const bool ok1 = j + 1 >= e && j + 1 < U.n && i <= j + 1;
+        for (int u = 0; u < 8; u += 2) {
+          const int j = j0 + c0 + u;
+          const bool ok0 = row_ok && j >= e && j < U.n && i <= j;
+          const bool ok1 = row_ok && j + 1 >= e && j + 1 < U.n && i <= j + 1;
           if (ok0 && ok1) {
-            *reinterpret_cast<double2*>(crow + j) = make_double2(v0, v1);
+            const double2 t = *reinterpret_cast<const double2*>(crow + j);
+            cv[u] = t.x;
+            cv[u + 1] = t.y;
           } else {
-            if (ok0) crow[j] = v0;
-            if (ok1) crow[j + 1] = v1;
+            cv[u] = ok0 ? crow[j] : 0.0;
+            cv[u + 1] = ok1 ? crow[j + 1] : 0.0;
           }
         }
-      }
+      };
+      double cur[8], nxt[8];
+      load_c(0, cur);
+      const uint32_t tacc = tmem + static_cast<uint32_t>(b * kUN) + (static_cast<uint32_t>(warp * 32) << 16);
+#pragma unroll 1
+      for (int c0 = 0; c0 < kUN; c0 += 8) {
+        uint32_t r[8];
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                     : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                       "=r"(r[7])
+                     : "r"(tacc + static_cast<uint32_t>(c0)));
+        if (c0 + 8 < kUN) load_c(c0 + 8, nxt);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        const int jb = j0 + c0;
+        const int js = min(max(jb, split_i0), U.n - 1);
+        const double unscale = 1.0 / (sa * U.b_scale[(js - split_i0) / kBM]);
+        if (row_ok) {
 #pragma unroll
-      for (int u = 0; u < 16; ++u) cur[u] = nxt[u];
+          for (int u = 0; u < 8; u += 2) {
+            const int j = jb + u;
+            const double v0 = cur[u] - static_cast<double>(__uint_as_float(r[u])) * unscale;
+            const double v1 = cur[u + 1] - static_cast<double>(__uint_as_float(r[u + 1])) * unscale;
+            const bool ok0 = j >= e && j < U.n && i <= j;
+            const bool ok1 = j + 1 >= e && j + 1 < U.n && i <= j + 1;
+            if (ok0 && ok1) {
+              *reinterpret_cast<double2*>(crow + j) = make_double2(v0, v1);
+            } else {
+              if (ok0) crow[j] = v0;
+              if (ok1) crow[j + 1] = v1;
+            }
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) cur[u] = nxt[u];
+      }
+      // this warp is done reading the accumulator
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(&accempty[b]));
     }
-    // every warp has read the accumulator before the next tile overwrites it
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();
   }
-  asm volatile("cp.async.wait_all;" ::: "memory");
-  if (!ok && threadIdx.x == 0) {
+  if (!ok) {
     atomicCAS(const_cast<int*>(&U.st->status), 0, BBK_ERR_TIMEOUT);
     atomicExch(const_cast<int*>(&U.st->abort), 1);
-    // let MMAs already issued finish before the accumulator is released (a
-    // bounded wait; the abort flag is set, so use a plain time bound)
-    if (committed >= 0) {
-      const uint32_t mb = smem_u32(&mbar[committed % S::kStages]);
-      const uint32_t par = static_cast<uint32_t>((committed / S::kStages) & 1);
-      const unsigned long long t0 = globaltimer_ns();
-      while (!mbar_try(mb, par) && globaltimer_ns() - t0 < timeout_ns) {
-      }
-    }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kUN) : "memory");
+  if (warp == kUWarps - 1)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * kUN) : "memory");
 }
 
 template <int kTerms>
@@ -1367,8 +1397,8 @@ int launch_umma_bf16(const UpdArgs& U, const __nv_bfloat16* ah, const __nv_bfloa
   const long long tm = (order + kUM - 1) / kUM + 1;
   const long long tiles = tm * (tm + 1) / 2;
   const int grid = static_cast<int>(std::max(1LL, std::min<long long>(tiles, 2LL * device_sm_count())));
-  umma_bf16s_update_kernel<kTerms><<<grid, kUThreads, S::kBytes, s>>>(U, ah, bh, kpad, term_stride,
-                                                                      wait_timeout_ns());
+  umma_bf16s_update_kernel<kTerms><<<grid, kUBlock, S::kBytes, s>>>(U, ah, bh, kpad, term_stride,
+                                                                    wait_timeout_ns());
   BBK_CUDA_TRY(cudaGetLastError());
   count_launch();
   return BBK_OK;
