@@ -66,7 +66,9 @@ def parse_args():
     ap.add_argument("--h", type=int, default=None, help="KKT: H block order (default 0.8 n)")
     ap.add_argument("--block", type=int, default=None)
     ap.add_argument("--nrhs", type=int, default=None)
-    ap.add_argument("--mode", default="fp64", choices=["fp64", "fp64_ordered", "fp32"])
+    ap.add_argument("--mode", default="fp64", choices=["fp64", "fp64_ordered", "fp32", "bf16x3", "bf16"],
+                    help="the FP64 line's trailing-update arithmetic (the low-precision modes are for "
+                         "profiling their update kernels: the line's solve is then unrefined)")
     ap.add_argument("--seed", type=int, default=20240)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -536,7 +538,8 @@ def run_main(args):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.mode != "fp32" else "f64+f32-update",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.mode in ("fp64", "fp64_ordered") else f"f64+{args.mode}-update",
         "data": f"synthetic: seeded {matrix_description(args.matrix, n, args.h)} (torch generators on the device)",
         "config": dict(workload_config(args), parallelism=f"replicas x{world} (one matrix per GPU)",
                        seed=args.seed,
