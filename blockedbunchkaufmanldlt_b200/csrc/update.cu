@@ -1027,37 +1027,102 @@ __global__ void __launch_bounds__(kThreadsMma) bf16s_update_kernel(UpdArgs U, co
   cp_async_wait<0>();
 }
 
+// The split operands in the tensor core's shared-memory order, for the
+// tcgen05 update: rows relative to t_i0 (the 128-aligned row at or below the
+// trailing matrix), in blocks of 128 rows x 16 k (2048 BF16 = 4 KB each,
+// block (rb, kc) at (rb * kpad / 16 + kc) * 2048), and inside a block the
+// K-major core-matrix layout the UMMA descriptors describe: element (r, k)
+// at (r / 8) * 128 + (k / 8) * 64 + (r % 8) * 8 + k % 8.  One bulk copy moves
+// a block into shared memory.  Rows outside [e, n) and k >= inner are zero.
+constexpr int kBlkRows = 128, kBlkK = 16, kBlkElems = kBlkRows * kBlkK;
+
+__device__ __forceinline__ size_t blocked_offset(int r, int k, int nkc) {
+  return static_cast<size_t>((r / kBlkRows) * nkc + k / kBlkK) * kBlkElems +
+         ((r % kBlkRows) / 8) * 128 + ((k % kBlkK) / 8) * 64 + (r % 8) * 8 + (k % 8);
+}
+
+template <int kTerms>
+__global__ void __launch_bounds__(256) split_blocked_kernel(UpdArgs U, __nv_bfloat16* ah, __nv_bfloat16* bh,
+                                                            int kpad, size_t term_stride) {
+  __shared__ double tile[kSplitTile][kSplitTile + 1];
+  if (!resolve_range(U)) return;  // U.tile_i0: the 64-aligned origin of the scales
+  const int t_i0 = (U.i_lo / kBlkRows) * kBlkRows;
+  const int rows = ((U.n - t_i0 + kBlkRows - 1) / kBlkRows) * kBlkRows;  // whole 128-row blocks
+  const int rt = rows / kSplitTile, kt = kpad / kSplitTile, nkc = kpad / kBlkK;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+  for (int blk = blockIdx.x; blk < 2 * rt * kt; blk += gridDim.x) {
+    const bool is_a = blk < rt * kt;
+    const int b2 = is_a ? blk : blk - rt * kt;
+    const int r0 = (b2 / kt) * kSplitTile, k0 = (b2 % kt) * kSplitTile;
+    // the 32 x 32 block (rows r0.., k k0..), scaled; A read along k, B along the rows
+    for (int yy = ty; yy < kSplitTile; yy += 8) {
+      int r, k;
+      if (is_a) {
+        r = r0 + yy;
+        k = k0 + tx;
+      } else {
+        r = r0 + tx;
+        k = k0 + yy;
+      }
+      const int c = t_i0 + r;
+      double v = 0.0;
+      if (c >= U.i_lo && c < U.n && k < U.inner) {
+        const double sc = (is_a ? U.a_scale : U.b_scale)[(c - U.tile_i0) / kBM];
+        v = sc * (is_a ? U.a[static_cast<long long>(c) * U.a_si + k] : U.b[static_cast<long long>(k) * U.b_sk + c]);
+      }
+      if (is_a)
+        tile[yy][tx] = v;  // [row][k]
+      else
+        tile[tx][yy] = v;
+    }
+    __syncthreads();
+    __nv_bfloat16* dst = is_a ? ah : bh;
+    for (int yy = ty; yy < kSplitTile; yy += 8) {
+      const int r = r0 + yy, k = k0 + tx;
+      float rest = static_cast<float>(tile[yy][tx]);
+      const size_t off = blocked_offset(r, k, nkc);
+#pragma unroll
+      for (int t = 0; t < kTerms; ++t) {
+        const __nv_bfloat16 h = __float2bfloat16_rn(rest);
+        dst[t * term_stride + off] = h;
+        rest -= __bfloat162float(h);
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // ---------------------------------------------------------------------------
 // BF16 update on the 5th-generation tensor cores (tcgen05 / UMMA).
 //
-// The split operands (split_kernel: kTerms scaled BF16 terms per operand, k
-// contiguous, zero-padded to kpad) are staged by cp.async into shared memory
-// in the no-swizzle K-major core-matrix layout (8 rows x 16 bytes per core
-// matrix; core matrices 128 bytes apart along k, 512 bytes apart along the
-// rows), and one thread issues tcgen05.mma.kind::f16 (M = N = 128, K = 16)
-// for every product t_a(A) t_b(B), a + b < kTerms, smallest first, into one
-// FP32 accumulator in tensor memory (128 lanes x 128 columns).  Completion is
-// tracked by tcgen05.commit on one mbarrier per stage; every wait is bounded
-// and a wait that runs out aborts the factorization with BBK_ERR_TIMEOUT.
-// The epilogue reads the accumulator with tcgen05.ld (warp w: lanes 32w..,
-// one C row per thread), unscales it and subtracts it from the FP64 trailing
-// matrix.  Two CTAs per SM, each with its own accumulator, so one CTA's
-// epilogue (the C traffic, which bounds this kernel) overlaps the other's
-// MMAs.
+// The split operands (split_blocked_kernel: kTerms scaled BF16 terms per
+// operand, stored in 4 KB blocks already in the shared-memory order of the
+// UMMA descriptors: no-swizzle K-major core matrices of 8 rows x 16 bytes,
+// 128 bytes apart along k and 256 bytes apart along the rows) are moved into
+// shared memory by bulk asynchronous copies, one per block, and one thread
+// issues tcgen05.mma.kind::f16 (M = N = 128, K = 16) for every product
+// t_a(A) t_b(B), a + b < kTerms, smallest first, into an FP32 accumulator in
+// tensor memory (128 lanes x 128 columns).  Completion is tracked by
+// mbarriers (transaction bytes for the copies, tcgen05.commit for the MMAs);
+// every wait is bounded and a wait that runs out aborts the factorization
+// with BBK_ERR_TIMEOUT.  The epilogue reads an accumulator with tcgen05.ld
+// (warp w: lanes 32w.., one C row per thread), unscales it and subtracts it
+// from the FP64 trailing matrix, while the other accumulator takes the next
+// tile's MMAs.  Two CTAs per SM.
 // ---------------------------------------------------------------------------
 constexpr int kUM = 128, kUN = 128;  // C tile
-constexpr int kUThreads = 128;        // 4 warps = the accumulator's 128 lanes
+
 
 // Per term count: the k chunk (BF16 elements) and the stages, sized so that
 // two CTAs fit one SM with the same bytes in flight (three terms: more,
 // shorter stages, so a stage is refilled soon after its MMAs finish).
 template <int kTerms>
 struct USmem {
-  static constexpr int kK = kTerms == 3 ? 16 : 32;
-  static constexpr int kOpBytes = kUM * kK * 2;  // one term of one operand per stage
+  static constexpr int kK = kBlkK;
+  static constexpr int kOpBytes = kUM * kK * 2;  // one term of one operand per stage: one 4 KB block
   static constexpr int kRowGroup = (kK / 8) * 128;  // bytes between 8-row core-matrix groups
   static constexpr int kStageBytes = 2 * kTerms * kOpBytes;
-  static constexpr int kStages = 4;
+  static constexpr int kStages = kTerms == 3 ? 4 : 8;
   // stages, then the barriers (2 x kStages + 4) and the accumulator address
   static constexpr size_t kBytes = static_cast<size_t>(kStages) * kStageBytes + 256;
   static_assert((2 * kStages + 4) * 8 + 4 <= 256, "barrier area");
@@ -1122,14 +1187,16 @@ __device__ bool mbar_wait(uint32_t mbar, uint32_t parity, const DeviceState* st,
 //   warps 0-3   epilogue: wait until an accumulator is full, read it with
 //               tcgen05.ld (warp w: lanes 32w..32w+31, one C row per
 //               thread), C -= unscale * acc, then mark the accumulator empty;
-//   warps 4-7   producers: cp.async the next chunk into a free stage and
-//               arrive on that stage's "full" barrier when the copies land;
-//   warp 8      lane 0 issues the MMAs of each full stage, commits them to
+//   warp 4      lane 0 moves the next chunk into a free stage with bulk
+//               asynchronous copies (one 4 KB block per operand and term,
+//               split_blocked_kernel's layout) that complete the stage's
+//               "full" barrier;
+//   warp 5      lane 0 issues the MMAs of each full stage, commits them to
 //               the stage's "empty" barrier and, after a tile's last chunk,
 //               to the accumulator's "full" barrier.
 // Two accumulators (2 x 128 TMEM columns) let the epilogue of one tile run
 // while the next tile's MMAs execute.
-constexpr int kUEpi = 4, kUProd = 4;
+constexpr int kUEpi = 4, kUProd = 1;
 constexpr int kUWarps = kUEpi + kUProd + 1;
 constexpr int kUBlock = kUWarps * 32;
 
@@ -1159,7 +1226,6 @@ __global__ void __launch_bounds__(kUBlock, 2) umma_bf16s_update_kernel(UpdArgs U
   const int inner = e - k0p;
   if (inner <= 0 || e >= U.n) return;
   const int split_i0 = (e / kBM) * kBM;
-  const int rows = U.n - split_i0;
   const int t_i0 = (e / kUM) * kUM;
   const int tm = (U.n - t_i0 + kUM - 1) / kUM;
   const int ntiles = tm * (tm + 1) / 2;
@@ -1176,8 +1242,7 @@ __global__ void __launch_bounds__(kUBlock, 2) umma_bf16s_update_kernel(UpdArgs U
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     if (lane == 0) {
       for (int st = 0; st < S::kStages; ++st) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&full[st])), "r"(kUProd * 32)
-                     : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&full[st])) : "memory");
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&empty[st])) : "memory");
       }
       for (int b = 0; b < 2; ++b) {
@@ -1202,43 +1267,41 @@ __global__ void __launch_bounds__(kUBlock, 2) umma_bf16s_update_kernel(UpdArgs U
   };
   bool ok = true;
 
-  if (warp >= kUEpi && warp < kUEpi + kUProd) {
-    // ---- producers
-    const int pt = threadIdx.x - kUEpi * 32;
-    constexpr int kCols = kUK / 8;     // 16-byte chunks per row
-    constexpr int kPer = kUM * kCols;  // 16-byte chunks per operand term
-    long long item = 0;
-    for (int m = 0; m < my_tiles && ok; ++m) {
-      int i0, j0;
-      tile_of(static_cast<int>(blockIdx.x) + m * static_cast<int>(gridDim.x), i0, j0);
-      for (int ch = 0; ch < nchunks; ++ch, ++item) {
-        const int st = static_cast<int>(item % S::kStages);
-        const long long use = item / S::kStages;
-        if (use >= 1 && !mbar_wait(smem_u32(&empty[st]), static_cast<uint32_t>((use - 1) & 1), U.st, timeout_ns)) {
-          ok = false;
-          break;
-        }
-        unsigned char* base = usm + st * S::kStageBytes;
-        // per operand and term, 128 rows x kUK k: row r's k-chunk c (8
-        // elements) at (r/8)*kRowGroup + c*128 + (r%8)*16
-        for (int q = pt; q < 2 * kTerms * kPer; q += kUProd * 32) {
-          const int blk = q / kPer, rem = q - blk * kPer;  // blk = op * kTerms + term
-          const int r = rem / kCols, c = rem % kCols;
-          const int op = blk / kTerms, term = blk - op * kTerms;
-          const int row = (op == 0 ? i0 : j0) - split_i0 + r;
-          const bool in = row >= 0 && row < rows;
-          const __nv_bfloat16* src = (op == 0 ? ah : bh) + term * term_stride +
-                                     static_cast<size_t>(in ? row : 0) * kpad + ch * kUK + c * 8;
-          const uint32_t dst =
-              smem_u32(base + blk * kUOpBytes + (r >> 3) * S::kRowGroup + c * 128 + (r & 7) * 16);
-          asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(in ? 16 : 0)
+  if (warp == kUEpi) {
+    // ---- producer: one thread moves each stage's 2 x kTerms blocks with
+    // bulk asynchronous copies that complete the stage's "full" barrier
+    if (lane == 0) {
+      const int nkc = kpad / kBlkK;
+      long long item = 0;
+      for (int m = 0; m < my_tiles && ok; ++m) {
+        int i0, j0;
+        tile_of(static_cast<int>(blockIdx.x) + m * static_cast<int>(gridDim.x), i0, j0);
+        const int rba = (i0 - t_i0) / kBlkRows, rbb = (j0 - t_i0) / kBlkRows;
+        for (int ch = 0; ch < nchunks; ++ch, ++item) {
+          const int st = static_cast<int>(item % S::kStages);
+          const long long use = item / S::kStages;
+          if (use >= 1 &&
+              !mbar_wait(smem_u32(&empty[st]), static_cast<uint32_t>((use - 1) & 1), U.st, timeout_ns)) {
+            ok = false;
+            break;
+          }
+          const uint32_t fb = smem_u32(&full[st]);
+          asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb), "r"(S::kStageBytes)
                        : "memory");
+          const uint32_t base = smem_u32(usm + st * S::kStageBytes);
+          for (int blk = 0; blk < 2 * kTerms; ++blk) {
+            const int op = blk / kTerms, term = blk - op * kTerms;
+            const __nv_bfloat16* src = (op == 0 ? ah : bh) + term * term_stride +
+                                       static_cast<size_t>((op == 0 ? rba : rbb) * nkc + ch) * kBlkElems;
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                    base + blk * kUOpBytes),
+                "l"(src), "r"(kUOpBytes), "r"(fb)
+                : "memory");
+          }
         }
-        asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(&full[st]))
-                     : "memory");
       }
     }
-    asm volatile("cp.async.wait_all;" ::: "memory");
   } else if (warp == kUWarps - 1) {
     // ---- MMA issue (one thread)
     if (lane == 0) {
@@ -1259,7 +1322,6 @@ __global__ void __launch_bounds__(kUBlock, 2) umma_bf16s_update_kernel(UpdArgs U
             ok = false;
             break;
           }
-          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // the copies, to the tensor core
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
           const uint32_t sb = smem_u32(usm + st * S::kStageBytes);
           for (int ia = kTerms - 1; ia >= 0; --ia)
@@ -1420,10 +1482,15 @@ int launch_bf16_split(const UpdArgs& U, __nv_bfloat16* buf, int kpad, size_t ter
   const int sms = device_sm_count();
   __nv_bfloat16* ah = buf;
   __nv_bfloat16* bh = buf + static_cast<size_t>(kTerms) * term_stride;
+  if (vec && use_umma_bf16() && kpad % kBlkK == 0) {
+    split_blocked_kernel<kTerms><<<4 * sms, 256, 0, s>>>(U, ah, bh, kpad, term_stride);
+    BBK_CUDA_TRY(cudaGetLastError());
+    count_launch();
+    return launch_umma_bf16<kTerms>(U, ah, bh, kpad, term_stride, order, s);
+  }
   split_kernel<kTerms><<<4 * sms, 256, 0, s>>>(U, ah, bh, kpad, term_stride);
   BBK_CUDA_TRY(cudaGetLastError());
   count_launch();
-  if (vec && use_umma_bf16()) return launch_umma_bf16<kTerms>(U, ah, bh, kpad, term_stride, order, s);
   const size_t bytes = HSmem<kTerms>::kBytes;
   static std::once_flag attr_once[64];
   int dev = 0;
