@@ -1123,13 +1123,11 @@ struct USmem {
   static constexpr int kRowGroup = (kK / 8) * 128;  // bytes between 8-row core-matrix groups
   static constexpr int kStageBytes = 2 * kTerms * kOpBytes;
   static constexpr int kStages = kTerms == 3 ? 4 : 8;
-  // stages, the epilogue's transpose tiles, then the barriers (2 x kStages
-  // + 4) and the accumulator address
-  static constexpr int kEpiBytes = 4 * 32 * 32 * 4;
-  static constexpr size_t kBytes = static_cast<size_t>(kStages) * kStageBytes + kEpiBytes + 256;
+  // stages, then the barriers (2 x kStages + 4) and the accumulator address
+  static constexpr size_t kBytes = static_cast<size_t>(kStages) * kStageBytes + 256;
   static_assert((2 * kStages + 4) * 8 + 4 <= 256, "barrier area");
 };
-static_assert(2 * (USmem<3>::kBytes + 1024) <= 228 * 1024, "two CTAs per SM");
+static_assert(2 * USmem<3>::kBytes + 2048 <= 228 * 1024, "two CTAs per SM");
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -1215,8 +1213,7 @@ __global__ void __launch_bounds__(kUBlock, 2) umma_bf16s_update_kernel(UpdArgs U
   constexpr int kUK = S::kK;
   constexpr int kUOpBytes = S::kOpBytes;
   extern __shared__ __align__(1024) unsigned char usm[];
-  float* epi = reinterpret_cast<float*>(usm + S::kStages * S::kStageBytes);  // kUEpi x 32 x 32 (transpose tiles)
-  uint64_t* full = reinterpret_cast<uint64_t*>(usm + S::kStages * S::kStageBytes + S::kEpiBytes);
+  uint64_t* full = reinterpret_cast<uint64_t*>(usm + S::kStages * S::kStageBytes);
   uint64_t* empty = full + S::kStages;
   uint64_t* accfull = empty + S::kStages;  // 2
   uint64_t* accempty = accfull + 2;        // 2
@@ -1372,53 +1369,61 @@ __global__ void __launch_bounds__(kUBlock, 2) umma_bf16s_update_kernel(UpdArgs U
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      // 32-column groups: the accumulator rows of this warp's 32 lanes go
-      // through a shared-memory tile (column index rotated by the row, so
-      // neither the row writes nor the column reads conflict), then each
-      // C row segment is read, updated and written by the whole warp as 256
-      // contiguous bytes
-      float* tr = epi + warp * 32 * 32;
-      const uint32_t tacc = tmem + static_cast<uint32_t>(b * kUN) + (static_cast<uint32_t>(warp * 32) << 16);
-      const int rbase = i0 + warp * 32;
-#pragma unroll 1
-      for (int c0 = 0; c0 < kUN; c0 += 32) {
-        uint32_t r[32];
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
-            "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-              "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]),
-              "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]),
-              "=r"(r[30]), "=r"(r[31])
-            : "r"(tacc + static_cast<uint32_t>(c0)));
-        // this lane's C column of the group, for all 32 rows (loads first)
-        const int j = j0 + c0 + lane;
-        const bool col_ok = j >= e && j < U.n;
-        double cv[32];
+      const int is = min(max(i, split_i0), U.n - 1);  // scale block of a row inside the matrix
+      const double sa = U.a_scale[(is - split_i0) / kBM];
+      double* crow = U.c + static_cast<long long>(is) * U.ldc;
+      // C values of the 8-column group at c0 (entries this thread does not
+      // update read as 0); the next group's load is in flight while a group
+      // is updated
+      auto load_c = [&](int c0, double (&cv)[8]) {
 #pragma unroll
-        for (int rr = 0; rr < 32; ++rr) {
-          const int ii = rbase + rr;
-          const bool ok = col_ok && ii >= e && ii < U.n && ii <= j;
-          cv[rr] = ok ? U.c[static_cast<long long>(ii) * U.ldc + j] : 0.0;
-        }
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-        for (int c = 0; c < 32; ++c) tr[lane * 32 + ((c + lane) & 31)] = __uint_as_float(r[c]);
-        __syncwarp();
-        const int js = min(max(j, split_i0), U.n - 1);
-        const double sb = U.b_scale[(js - split_i0) / kBM];
-#pragma unroll
-        for (int rr = 0; rr < 32; ++rr) {
-          const int ii = rbase + rr;
-          const bool ok = col_ok && ii >= e && ii < U.n && ii <= j;
-          if (ok) {
-            const double sa = U.a_scale[(ii - split_i0) / kBM];
-            const double v = static_cast<double>(tr[rr * 32 + ((lane + rr) & 31)]);
-            U.c[static_cast<long long>(ii) * U.ldc + j] = cv[rr] - v / (sa * sb);
+        for (int u = 0; u < 8; u += 2) {
+          const int j = j0 + c0 + u;
+          const bool ok0 = row_ok && j >= e && j < U.n && i <= j;
+          const bool ok1 = row_ok && j + 1 >= e && j + 1 < U.n && i <= j + 1;
+          if (ok0 && ok1) {
+            const double2 t = *reinterpret_cast<const double2*>(crow + j);
+            cv[u] = t.x;
+            cv[u + 1] = t.y;
+          } else {
+            cv[u] = ok0 ? crow[j] : 0.0;
+            cv[u + 1] = ok1 ? crow[j + 1] : 0.0;
           }
         }
-        __syncwarp();  // the tile is rewritten by the next group
+      };
+      double cur[8], nxt[8];
+      load_c(0, cur);
+      const uint32_t tacc = tmem + static_cast<uint32_t>(b * kUN) + (static_cast<uint32_t>(warp * 32) << 16);
+#pragma unroll 1
+      for (int c0 = 0; c0 < kUN; c0 += 8) {
+        uint32_t r[8];
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                     : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                       "=r"(r[7])
+                     : "r"(tacc + static_cast<uint32_t>(c0)));
+        if (c0 + 8 < kUN) load_c(c0 + 8, nxt);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        const int jb = j0 + c0;
+        const int js = min(max(jb, split_i0), U.n - 1);
+        const double unscale = 1.0 / (sa * U.b_scale[(js - split_i0) / kBM]);
+        if (row_ok) {
+#pragma unroll
+          for (int u = 0; u < 8; u += 2) {
+            const int j = jb + u;
+            const double v0 = cur[u] - static_cast<double>(__uint_as_float(r[u])) * unscale;
+            const double v1 = cur[u + 1] - static_cast<double>(__uint_as_float(r[u + 1])) * unscale;
+            const bool ok0 = j >= e && j < U.n && i <= j;
+            const bool ok1 = j + 1 >= e && j + 1 < U.n && i <= j + 1;
+            if (ok0 && ok1) {
+              *reinterpret_cast<double2*>(crow + j) = make_double2(v0, v1);
+            } else {
+              if (ok0) crow[j] = v0;
+              if (ok1) crow[j + 1] = v1;
+            }
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) cur[u] = nxt[u];
       }
       // this warp is done reading the accumulator
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
