@@ -94,19 +94,20 @@ __device__ __forceinline__ double div_or_zero(double x, double den) {
   return den == 0.0 ? 0.0 : xdiv(x, den);
 }
 
-// sum_{q < count} c[q] * w(q) in ascending q, every product and sum rounded
-// separately (the reference's order).  The products do not depend on the
-// running sum: each batch of eight is loaded and multiplied while the
-// previous batch is being added.
+// acc + sum_{q0 <= q < q1} c[q] * w(q) in ascending q, every product and sum
+// rounded separately (the reference's order: its sums start at 0.0 and add
+// one product at a time, so a sum over [0, q1) split at any q0 and continued
+// from the first part's result is the same sum bit for bit).  The products
+// do not depend on the running sum: each batch of eight is loaded and
+// multiplied while the previous batch is being added.
 template <typename WGet>
-__device__ __forceinline__ double ordered_dot(const double* c, int count, WGet&& w) {
-  double acc = 0.0;
-  int q = 0;
-  if (count >= 8) {
+__device__ __forceinline__ double ordered_dot_range(double acc, const double* c, int q0, int q1, WGet&& w) {
+  int q = q0;
+  if (q1 - q0 >= 8) {
     double cur[8];
 #pragma unroll
-    for (int u = 0; u < 8; ++u) cur[u] = xmul(c[u], w(u));
-    for (q = 8; q + 8 <= count; q += 8) {
+    for (int u = 0; u < 8; ++u) cur[u] = xmul(c[q0 + u], w(q0 + u));
+    for (q = q0 + 8; q + 8 <= q1; q += 8) {
       double nxt[8];
 #pragma unroll
       for (int u = 0; u < 8; ++u) nxt[u] = xmul(c[q + u], w(q + u));
@@ -118,19 +119,25 @@ __device__ __forceinline__ double ordered_dot(const double* c, int count, WGet&&
 #pragma unroll
     for (int u = 0; u < 8; ++u) acc = xadd(acc, cur[u]);
   }
-  for (; q < count; ++q) acc = xadd(acc, xmul(c[q], w(q)));
+  for (; q < q1; ++q) acc = xadd(acc, xmul(c[q], w(q)));
   return acc;
 }
 
-// Two sums over the same w(q) at once: s1 = sum c1[q] w(q), s2 = sum c2[q] w(q),
-// each added in ascending q with every product and sum rounded separately,
-// so each is bitwise ordered_dot of its coefficients; w(q) is read once.
 template <typename WGet>
-__device__ __forceinline__ void ordered_dot2(const double* c1, const double* c2, int count, WGet&& w,
-                                             double& s1, double& s2) {
-  double a1 = 0.0, a2 = 0.0;
-  int q = 0;
-  for (; q + 4 <= count; q += 4) {
+__device__ __forceinline__ double ordered_dot(const double* c, int count, WGet&& w) {
+  return ordered_dot_range(0.0, c, 0, count, w);
+}
+
+// Two sums over the same w(q) at once, continued from s1 / s2: s1 += sum
+// c1[q] w(q), s2 += sum c2[q] w(q), q in [q0, q1), each added in ascending q
+// with every product and sum rounded separately, so each is bitwise
+// ordered_dot of its coefficients; w(q) is read once.
+template <typename WGet>
+__device__ __forceinline__ void ordered_dot2_range(const double* c1, const double* c2, int q0, int q1, WGet&& w,
+                                                   double& s1, double& s2) {
+  double a1 = s1, a2 = s2;
+  int q = q0;
+  for (; q + 4 <= q1; q += 4) {
     double p1[4], p2[4];
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
@@ -144,7 +151,7 @@ __device__ __forceinline__ void ordered_dot2(const double* c1, const double* c2,
       a2 = xadd(a2, p2[u]);
     }
   }
-  for (; q < count; ++q) {
+  for (; q < q1; ++q) {
     const double x = w(q);
     a1 = xadd(a1, xmul(c1[q], x));
     a2 = xadd(a2, xmul(c2[q], x));
@@ -153,13 +160,22 @@ __device__ __forceinline__ void ordered_dot2(const double* c1, const double* c2,
   s2 = a2;
 }
 
-// The reassociated counterpart of ordered_dot2: four FMA accumulators per sum.
 template <typename WGet>
-__device__ __forceinline__ void split_dot2(const double* c1, const double* c2, int count, WGet&& w,
-                                           double& s1, double& s2) {
+__device__ __forceinline__ void ordered_dot2(const double* c1, const double* c2, int count, WGet&& w,
+                                             double& s1, double& s2) {
+  s1 = 0.0;
+  s2 = 0.0;
+  ordered_dot2_range(c1, c2, 0, count, w, s1, s2);
+}
+
+// The reassociated counterpart of ordered_dot2: four FMA accumulators per
+// sum over q in [q0, q1).
+template <typename WGet>
+__device__ __forceinline__ void split_dot2_range(const double* c1, const double* c2, int q0, int q1, WGet&& w,
+                                                 double& s1, double& s2) {
   double a[4] = {0.0, 0.0, 0.0, 0.0}, b[4] = {0.0, 0.0, 0.0, 0.0};
-  int q = 0;
-  for (; q + 4 <= count; q += 4) {
+  int q = q0;
+  for (; q + 4 <= q1; q += 4) {
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       const double x = w(q + u);
@@ -169,7 +185,7 @@ __device__ __forceinline__ void split_dot2(const double* c1, const double* c2, i
   }
 #pragma unroll
   for (int u = 0; u < 4; ++u)
-    if (q + u < count) {
+    if (q + u < q1) {
       const double x = w(q + u);
       a[u] = __fma_rn(c1[q + u], x, a[u]);
       b[u] = __fma_rn(c2[q + u], x, b[u]);
@@ -178,22 +194,33 @@ __device__ __forceinline__ void split_dot2(const double* c1, const double* c2, i
   s2 = (b[0] + b[1]) + (b[2] + b[3]);
 }
 
-// sum_{q < count} c[q] * w(q) with eight independent FMA accumulators
+template <typename WGet>
+__device__ __forceinline__ void split_dot2(const double* c1, const double* c2, int count, WGet&& w,
+                                           double& s1, double& s2) {
+  split_dot2_range(c1, c2, 0, count, w, s1, s2);
+}
+
+// sum_{q0 <= q < q1} c[q] * w(q) with eight independent FMA accumulators
 // combined pairwise: the same sum, reassociated, with an eighth of the
 // dependent-latency chain (update modes that do not reproduce the
 // reference's rounding).
 template <typename WGet>
-__device__ __forceinline__ double split_dot(const double* c, int count, WGet&& w) {
+__device__ __forceinline__ double split_dot_range(const double* c, int q0, int q1, WGet&& w) {
   double a[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  int q = 0;
-  for (; q + 8 <= count; q += 8) {
+  int q = q0;
+  for (; q + 8 <= q1; q += 8) {
 #pragma unroll
     for (int u = 0; u < 8; ++u) a[u] = __fma_rn(c[q + u], w(q + u), a[u]);
   }
 #pragma unroll
   for (int u = 0; u < 8; ++u)
-    if (q + u < count) a[u] = __fma_rn(c[q + u], w(q + u), a[u]);
+    if (q + u < q1) a[u] = __fma_rn(c[q + u], w(q + u), a[u]);
   return ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
+}
+
+template <typename WGet>
+__device__ __forceinline__ double split_dot(const double* c, int count, WGet&& w) {
+  return split_dot_range(c, 0, count, w);
 }
 
 // Device status words shared by every kernel of one factorization.

@@ -97,6 +97,8 @@ struct PanelArgs {
   int coef_cap;      // doubles reserved for each coefficient column
   int w_smem;        // keep this CTA's panel rows in shared memory
   int smem_cols;     // slice width the shared-memory allocation holds
+  int wcap;          // doubles of shared memory for panel rows: all of them (w_smem), else the
+                     // first wcap / S rows of the slice (the rest in wslot)
   unsigned long long* stats;  // optional per-phase nanoseconds (CTA 0)
   unsigned poll_ns;           // pause between polls of the arrival counter
   double* pivlog;             // optional decision log, kPivLogWords per position
@@ -373,21 +375,27 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
   const int ldu = P.ldu;
   auto owner = [&](int z) -> int { return (z - kstart) / S; };
   // shared memory: two coefficient columns, candidate column and row computed
-  // ahead of this CTA's slots,
-  // (when it fits) the slots' panel rows wsm[m*S + (z - lo)], then the maps
+  // ahead of this CTA's slots, the per-warp partial sums, the slots' panel
+  // rows wsm[m*S + (z - lo)] (all of them, or the first srows), then the maps
   double* coef = dsm;
   double* coef2 = dsm + P.coef_cap;  // coefficients of a row computed ahead
   double* wcs = dsm + 2 * P.coef_cap;
   double* svs = wcs + P.smem_cols;   // the row computed ahead, by slot
   double* wpart = svs + P.smem_cols;  // per-warp partial sums: 2 x kWarps x kPairSlots
-  double* wsm = wpart + 2 * kWarps * kPairSlots;
-  int* win = reinterpret_cast<int*>(
-      wsm + (kSmemW ? static_cast<size_t>(P.win_rows) * P.smem_cols : 0));
+  double* wsm = wpart + 2 * kWarps * kPairSlots;  // wcap doubles
+  int* win = reinterpret_cast<int*>(wsm + P.wcap);
   int* mypos = win + P.win_pad;  // index held by slot lo + zz
+  // panel rows kept in shared memory: all of them, or as many rows of this
+  // panel's slot width as the allocation holds
+  const int srows = kSmemW ? P.win_rows : min(P.win_rows, P.wcap / max(S, 1));
   auto wat = [&](int m, int z) -> double& {
-    if (kSmemW) return wsm[m * S + (z - lo)];
+    if (kSmemW || m < srows) return wsm[m * S + (z - lo)];
     return P.wslot[m * ldw + z];
   };
+  // the same, split by where the rows live (the hot dot products run over
+  // the shared-memory rows and then the global ones)
+  auto wat_s = [&](int m, int z) -> double { return wsm[m * S + (z - lo)]; };
+  auto wat_g = [&](int m, int z) -> double { return P.wslot[m * ldw + z]; };
   // A(x, z) of the symmetric matrix from its upper triangle (A is not written
   // while the panel runs)
   auto asym = [&](int x, int z) -> double {
@@ -416,7 +424,7 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
     const int x = kstart + m, z = lo + zz;
     const double* src = x <= z ? P.a + static_cast<long long>(x) * lda + z
                                : P.a + static_cast<long long>(z) * lda + x;
-    if (kSmemW)
+    if (kSmemW || m < srows)
       cp_async_8(&wsm[m * S + zz], src);
     else
       P.wslot[m * ldw + z] = __ldg(src);
@@ -515,14 +523,19 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
           const int w = t >> 5, ln = t & 31;
           const int qa = (lp * w) / kWarps, qb = (lp * (w + 1)) / kWarps;
           double s1[3] = {0.0, 0.0, 0.0};
-          for (int q = qa; q < qb; ++q) {
-            const double c1 = coef[q];
+          auto rows = [&](int q0, int q1, auto&& wget) {
+            for (int q = q0; q < q1; ++q) {
+              const double c1 = coef[q];
 #pragma unroll
-            for (int k = 0; k < 3; ++k) {
-              const int zz = ln + 32 * k;
-              if (zz < width) s1[k] = __fma_rn(c1, wat(q, lo + zz), s1[k]);
+              for (int k = 0; k < 3; ++k) {
+                const int zz = ln + 32 * k;
+                if (zz < width) s1[k] = __fma_rn(c1, wget(q, lo + zz), s1[k]);
+              }
             }
-          }
+          };
+          const int qm = kSmemW ? qb : min(max(qa, srows), qb);
+          rows(qa, qm, wat_s);
+          if (!kSmemW) rows(qm, qb, wat_g);
 #pragma unroll
           for (int k = 0; k < 3; ++k) {
             const int zz = ln + 32 * k;
@@ -546,8 +559,17 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
           if (z < hi) {
             const int j = mypos[z - lo];
             if (j >= p) {
-              const double acc = kOrdered ? ordered_dot(coef, lp, [&](int q) { return wat(q, z); })
-                                          : split_dot(coef, lp, [&](int q) { return wat(q, z); });
+              double acc;
+              if (kSmemW) {
+                acc = kOrdered ? ordered_dot(coef, lp, [&](int q) { return wat(q, z); })
+                               : split_dot(coef, lp, [&](int q) { return wat(q, z); });
+              } else {
+                const int qs = min(lp, srows);
+                auto ws = [&](int q) { return wat_s(q, z); };
+                auto wg = [&](int q) { return wat_g(q, z); };
+                acc = kOrdered ? ordered_dot_range(ordered_dot_range(0.0, coef, 0, qs, ws), coef, qs, lp, wg)
+                               : split_dot_range(coef, 0, qs, ws) + split_dot_range(coef, qs, lp, wg);
+              }
               finish_row(z, j, av[k], acc);
             }
           }
@@ -700,18 +722,23 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
           const int w = t >> 5, ln = t & 31;
           const int qa = (lp * w) / kWarps, qb = (lp * (w + 1)) / kWarps;
           double sa[3] = {0.0, 0.0, 0.0}, sb[3] = {0.0, 0.0, 0.0};
-          for (int q = qa; q < qb; ++q) {
-            const double c1 = coef[q], c2 = coef2[q];
+          auto rows = [&](int q0, int q1, auto&& wget) {
+            for (int q = q0; q < q1; ++q) {
+              const double c1 = coef[q], c2 = coef2[q];
 #pragma unroll
-            for (int k = 0; k < 3; ++k) {
-              const int zz = ln + 32 * k;
-              if (zz < width) {
-                const double x = wat(q, lo + zz);
-                sa[k] = __fma_rn(c1, x, sa[k]);
-                sb[k] = __fma_rn(c2, x, sb[k]);
+              for (int k = 0; k < 3; ++k) {
+                const int zz = ln + 32 * k;
+                if (zz < width) {
+                  const double x = wget(q, lo + zz);
+                  sa[k] = __fma_rn(c1, x, sa[k]);
+                  sb[k] = __fma_rn(c2, x, sb[k]);
+                }
               }
             }
-          }
+          };
+          const int qm = kSmemW ? qb : min(max(qa, srows), qb);
+          rows(qa, qm, wat_s);
+          if (!kSmemW) rows(qm, qb, wat_g);
 #pragma unroll
           for (int k = 0; k < 3; ++k) {
             const int zz = ln + 32 * k;
@@ -744,13 +771,37 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
               const bool two = spec && i > p;
               double acc, part = 0.0;
               auto wq = [&](int q) { return wat(q, z); };
-              if (two) {
-                if (kOrdered)
-                  ordered_dot2(coef, coef2, lp, wq, acc, part);
-                else
-                  split_dot2(coef, coef2, lp, wq, acc, part);
+              if (kSmemW) {
+                if (two) {
+                  if (kOrdered)
+                    ordered_dot2(coef, coef2, lp, wq, acc, part);
+                  else
+                    split_dot2(coef, coef2, lp, wq, acc, part);
+                } else {
+                  acc = kOrdered ? ordered_dot(coef, lp, wq) : split_dot(coef, lp, wq);
+                }
               } else {
-                acc = kOrdered ? ordered_dot(coef, lp, wq) : split_dot(coef, lp, wq);
+                // shared-memory rows first, then the global ones (the
+                // ordered mode continues the same sums: same order)
+                const int qs = min(lp, srows);
+                auto ws = [&](int q) { return wat_s(q, z); };
+                auto wg = [&](int q) { return wat_g(q, z); };
+                if (two) {
+                  if (kOrdered) {
+                    acc = 0.0;
+                    ordered_dot2_range(coef, coef2, 0, qs, ws, acc, part);
+                    ordered_dot2_range(coef, coef2, qs, lp, wg, acc, part);
+                  } else {
+                    double a2, p2;
+                    split_dot2_range(coef, coef2, 0, qs, ws, acc, part);
+                    split_dot2_range(coef, coef2, qs, lp, wg, a2, p2);
+                    acc += a2;
+                    part += p2;
+                  }
+                } else {
+                  acc = kOrdered ? ordered_dot_range(ordered_dot_range(0.0, coef, 0, qs, ws), coef, qs, lp, wg)
+                                 : split_dot_range(coef, 0, qs, ws) + split_dot_range(coef, qs, lp, wg);
+                }
               }
               finish(z, i, acc, part, two);
             }
@@ -1257,8 +1308,8 @@ int launch_panel(const FactorPlan& plan, int panel, cudaStream_t s) {
   if (plan.grid > kMaxGrid)
     return set_error(BBK_ERR_INVALID_ARGUMENT, "panel grid %d exceeds %d", plan.grid, kMaxGrid);
   // shared memory: two coefficient columns + candidate column + row computed
-  // ahead + (if it fits) the
-  // slots' panel rows, then the window map and the slot -> index map
+  // ahead + per-warp partial sums + the slots' panel rows (all, or as many
+  // as fit), then the window map and the slot -> index map
   const int smax = (plan.n + plan.grid - 1) / plan.grid;
   P.coef_cap = static_cast<int>(align_up(static_cast<size_t>(plan.b) + 4, 2));
   P.smem_cols = smax;
@@ -1268,7 +1319,22 @@ int launch_panel(const FactorPlan& plan, int panel, cudaStream_t s) {
   const size_t wbytes = static_cast<size_t>(P.win_rows) * smax * sizeof(double);
   const size_t limit = 220 * 1024;
   P.w_smem = base + wbytes <= limit;
-  const size_t bytes = base + (P.w_smem ? wbytes : 0);
+  // a slice too wide for shared memory keeps its first rows there (the rows
+  // every pivot step of the panel reads) and the rest in global memory; the
+  // kernel divides the room by its own slot width, which shrinks as the
+  // factorization proceeds
+  size_t wroom = P.w_smem ? wbytes : (base < limit ? (limit - base) & ~static_cast<size_t>(7) : 0);
+  if (const char* e = getenv("BBK_PANEL_SMEM_ROWS")) {
+    // testing and tuning: at most this many rows of the widest slice in
+    // shared memory (the split layout at any size)
+    const size_t cap = static_cast<size_t>(std::max(0, atoi(e))) * smax * sizeof(double);
+    if (cap < wroom) {
+      P.w_smem = 0;
+      wroom = cap;
+    }
+  }
+  P.wcap = static_cast<int>(wroom / sizeof(double));
+  const size_t bytes = base + wroom;
   const bool ordered = plan.mode == BBK_UPDATE_FP64_ORDERED;
   const void* fn = ordered ? (P.w_smem ? reinterpret_cast<const void*>(panel_kernel<true, true>)
                                        : reinterpret_cast<const void*>(panel_kernel<true, false>))

@@ -122,6 +122,26 @@ def test_boundary_shifts_bitwise_ordered(cuda, bbk, port, n, b, seed):
     assert any(e != min(n, (k + 1) * b) for k, e in enumerate(want.panel_end))  # shifts happen
 
 
+@pytest.mark.parametrize("rows", [0, 7, 40])
+def test_split_panel_rows_bitwise_ordered(cuda, bbk, port, monkeypatch, rows):
+    # A slice too wide for shared memory keeps its first rows there and the
+    # rest in global memory; BBK_PANEL_SMEM_ROWS forces that split at a small
+    # size.  The ordered mode continues each sum across the split, so it must
+    # stay the reference bit for bit; the reassociated mode must take the
+    # same pivots.
+    monkeypatch.setenv("BBK_PANEL_SMEM_ROWS", str(rows))
+    for a, b in ((kkt_matrix(1200, 960, 1205), 64), (uniform_symmetric(1100, 78), 40)):
+        want = port.factor(a, b)
+        got = bbk.factor_host(a, b, mode="fp64_ordered")
+        assert np.array_equal(np.triu(got.factors), np.triu(want.factors)), (rows, b)
+        assert np.array_equal(got.perm, want.perm) and np.array_equal(got.pivot_types, want.pivot_types)
+        assert np.array_equal(got.panel_end, want.panel_end)
+        fast = bbk.factor_host(a, b, mode="fp64")
+        assert np.array_equal(fast.pivot_types, want.pivot_types) and np.array_equal(fast.perm, want.perm)
+        res = relative_error(reconstruct(fast.factors, fast.perm, fast.pivot_types), a)
+        assert res < TOLERANCE, res
+
+
 def test_scale_sweep(cuda, bbk, port):
     # tests/block_ldlt_decomposition_test.cc:40-99: value scales 1e-12 .. 1e12
     scales = [1e-12, 1e-9, 1e-6, 1e-3, 1.0, 1e3, 1e6, 1e9, 1e12]
