@@ -25,6 +25,36 @@ def test_solve_matches_oracle(cuda, bbk, port, n, b, nrhs):
     assert backward_error(a, got, rhs) < 1e-14
 
 
+@pytest.mark.parametrize("n,b", [(9600, 64), (20000, 128)])
+def test_pull_sweep_agrees_with_streaming_sweep(cuda, bbk, n, b):
+    # Up to 32 right-hand sides go through the pull sweep (8 per launch: each
+    # CTA gathers the solved blocks' contributions for its next block); more
+    # go through the streaming sweep (each solved block pushed into every
+    # later block).  The two sum in different orders, so they agree to
+    # rounding: columns solved among 160 against the same columns solved
+    # among 4 (one launch) and 12 (two launches), each with a backward error
+    # at the FP64 level.  n=9600 and 20000 give 2 and 3 blocks per CTA.
+    import torch
+    g = torch.Generator(device=cuda).manual_seed(n)
+    a = torch.rand(n, n, device=cuda, dtype=torch.float64, generator=g) * 2 - 1
+    a = a + a.T
+    f = a.clone()
+    perm, pt, _ = bbk.factor_device(f, b, mode="fp64")
+    rhs = torch.randn(160, n, device=cuda, dtype=torch.float64, generator=g)
+    many = bbk.solve_device(f, perm, pt, rhs.clone())
+
+    def berr(x, r):
+        res = a @ x.T - r.T
+        return float(res.abs().max() / (a.abs().sum(1).max() * x.abs().max() + r.abs().max()))
+
+    assert berr(many[:12], rhs[:12]) < 1e-14
+    for k in (4, 12):
+        few = bbk.solve_device(f, perm, pt, rhs[:k].clone())
+        assert berr(few, rhs[:k]) < 1e-14, k
+        diff = float((many[:k] - few).abs().max() / many[:k].abs().max())
+        assert diff < 1e-9, (k, diff)
+
+
 def test_factor_solve_one_call_kkt(cuda, bbk):
     a = kkt_matrix(1200, 960, seed=5)
     rhs = np.random.default_rng(1).standard_normal(1200)
