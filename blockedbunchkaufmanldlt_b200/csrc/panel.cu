@@ -1116,6 +1116,8 @@ struct FinArgs {
 };
 
 constexpr int kFinTile = 32;
+constexpr int kFinUnroll = 4;  // loads in flight per thread in the write-back loops
+constexpr int kFinCtasPerSm = 6;  // resident at 40 registers per thread
 __global__ void __launch_bounds__(256) finalize_kernel(FinArgs F) {
   __shared__ double tile[kFinTile][kFinTile + 1];
   if (ld_relaxed_s32(&F.st->abort)) return;
@@ -1131,21 +1133,46 @@ __global__ void __launch_bounds__(256) finalize_kernel(FinArgs F) {
   const int cnt = ldcg(&F.st->moved[F.panel & 1]);
   const int* list = F.moved + (F.panel & 1) * F.move_cap;
   if (cnt > 0) {
-    const long long m = n - e;
-    for (long long idx = gtid; idx < cnt * m; idx += nthreads) {
-      const int ix = static_cast<int>(idx / m);
-      const int x = list[ix];
-      if (x < e) continue;
-      const int y = e + static_cast<int>(idx - ix * m);
-      const double v = F.gbuf[ix * F.ldg + (y - k0)];
-      if (x <= y)
-        F.a[static_cast<long long>(x) * lda + y] = v;
-      else
-        F.a[static_cast<long long>(y) * lda + x] = v;
+    // each thread keeps kFinUnroll loads in flight before its stores
+    const long long m = n - e, total1 = cnt * m, total2 = static_cast<long long>(k0) * cnt;
+    for (long long base = gtid; base < total1; base += nthreads * kFinUnroll) {
+      double v[kFinUnroll];
+      long long dst[kFinUnroll];
+#pragma unroll
+      for (int u = 0; u < kFinUnroll; ++u) {
+        const long long idx = base + u * nthreads;
+        dst[u] = -1;
+        v[u] = 0.0;
+        if (idx < total1) {
+          const int ix = static_cast<int>(idx / m), y = e + static_cast<int>(idx - ix * m);
+          const int x = list[ix];
+          if (x >= e) {
+            v[u] = F.gbuf[ix * F.ldg + (y - k0)];
+            dst[u] = x <= y ? static_cast<long long>(x) * lda + y : static_cast<long long>(y) * lda + x;
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kFinUnroll; ++u)
+        if (dst[u] >= 0) F.a[dst[u]] = v[u];
     }
-    for (long long idx = gtid; idx < static_cast<long long>(k0) * cnt; idx += nthreads) {
-      const int q = static_cast<int>(idx / cnt), ix = static_cast<int>(idx - static_cast<long long>(q) * cnt);
-      F.a[static_cast<long long>(q) * lda + list[ix]] = F.gbuf2[static_cast<long long>(q) * F.move_cap + ix];
+    for (long long base = gtid; base < total2; base += nthreads * kFinUnroll) {
+      double v[kFinUnroll];
+      long long dst[kFinUnroll];
+#pragma unroll
+      for (int u = 0; u < kFinUnroll; ++u) {
+        const long long idx = base + u * nthreads;
+        dst[u] = -1;
+        v[u] = 0.0;
+        if (idx < total2) {
+          const int q = static_cast<int>(idx / cnt), ix = static_cast<int>(idx - static_cast<long long>(q) * cnt);
+          v[u] = F.gbuf2[static_cast<long long>(q) * F.move_cap + ix];
+          dst[u] = static_cast<long long>(q) * lda + list[ix];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kFinUnroll; ++u)
+        if (dst[u] >= 0) F.a[dst[u]] = v[u];
     }
     for (long long ix = gtid; ix < cnt; ix += nthreads) F.perm[list[ix]] = F.permbuf[ix];
   }
@@ -1393,7 +1420,11 @@ int launch_finalize(const FactorPlan& plan, int panel, cudaStream_t s) {
   F.n = plan.n;
   F.st = plan.state;
   F.panel = panel;
-  finalize_kernel<<<2 * sms, 256, 0, s>>>(F);
+  // large orders: a full SM of threads (n=40000: 38.4 -> 35.1 ms per
+  // factorization); small ones keep 2 CTAs per SM (n=10000: 1.06 ms, 1.12
+  // with the full grid)
+  const int ctas = (plan.n >= 16384 ? kFinCtasPerSm : 2) * sms;
+  finalize_kernel<<<ctas, 256, 0, s>>>(F);
   BBK_CUDA_TRY(cudaGetLastError());
   count_launch();
   return BBK_OK;
