@@ -263,6 +263,7 @@ int launch_init(int n, int* perm, int* pivot_types, DeviceState* st,
                 unsigned long long* slots, size_t slot_words, cudaStream_t s);
 int launch_panel(const FactorPlan& plan, int panel, cudaStream_t s);
 int launch_finalize(const FactorPlan& plan, int panel, cudaStream_t s);
+int launch_left_swaps(const FactorPlan& plan, cudaStream_t s);
 int launch_wrows(const FactorPlan& plan, int panel, cudaStream_t s);
 int launch_update(const FactorPlan& plan, int panel, cudaStream_t s);
 int launch_status_copy(const DeviceState* st, int* status_out, cudaStream_t s);
@@ -327,7 +328,11 @@ struct FactorPlan {
   int* moved = nullptr;      // 2 x move_cap: indices a panel's interchanges moved
   int move_cap = 0;
   double* gbuf = nullptr;    // move_cap x ldw: gathered rows of the moved indices
-  double* gbuf2 = nullptr;   // n x move_cap: factored rows at the moved columns
+  int* moves = nullptr;      // nb x 2 x move_cap: each panel's moves (positions dst, then src)
+  int* move_counts = nullptr;  // nb: moves per panel
+  int* bounds = nullptr;     // 2 nb: each panel's [start, end)
+  int* posinv = nullptr;     // n: position at the end of a panel -> final position
+  int* movetmp = nullptr;    // move_cap + 2
   int* permbuf = nullptr;    // move_cap: gathered permutation entries
   unsigned long long* slots = nullptr;  // 2 x grid x kSlotWords
   DeviceState* state = nullptr;

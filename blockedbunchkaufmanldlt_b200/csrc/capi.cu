@@ -88,7 +88,12 @@ size_t carve_factor(FactorPlan& plan, char* base) {
   plan.move_cap = static_cast<int>(align_up(2 * static_cast<size_t>(b) + 4, 4));
   plan.moved = c.take<int>(2 * static_cast<size_t>(plan.move_cap));
   plan.gbuf = c.take<double>(static_cast<size_t>(plan.move_cap) * npad);
-  plan.gbuf2 = c.take<double>(static_cast<size_t>(npad) * plan.move_cap);
+  const size_t nb = (static_cast<size_t>(n) + b - 1) / b;
+  plan.moves = c.take<int>(nb * 2 * plan.move_cap);
+  plan.move_counts = c.take<int>(nb);
+  plan.bounds = c.take<int>(2 * nb);
+  plan.posinv = c.take<int>(static_cast<size_t>(npad));
+  plan.movetmp = c.take<int>(static_cast<size_t>(plan.move_cap) + 2);
   plan.permbuf = c.take<int>(static_cast<size_t>(plan.move_cap));
   plan.scales = c.take<double>(2 * (static_cast<size_t>(n) / 64 + 2));
   plan.kpad = static_cast<int>(align_up(static_cast<size_t>(b) + 1, 32));
@@ -202,6 +207,7 @@ static int enqueue_factor(FactorPlan& plan, int* status_device, cudaStream_t s) 
     if (plan.wrows && (rc = launch_wrows(plan, panel, s))) return rc;
     if ((rc = profiled(kProfUpdate, s, [&] { return launch_update(plan, panel, s); }))) return rc;
   }
+  if ((rc = profiled(kProfFinalize, s, [&] { return launch_left_swaps(plan, s); }))) return rc;
   return launch_status_copy(plan.state, status_device, s);
 }
 

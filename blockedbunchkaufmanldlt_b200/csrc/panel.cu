@@ -84,7 +84,9 @@ struct PanelArgs {
   int* moved;        // 2 x move_cap
   int move_cap;
   double* gbuf;      // move_cap x ldw
-  double* gbuf2;     // n x move_cap
+  int* moves;        // nb x 2 x move_cap: each panel's moves, for the deferred column exchanges
+  int* move_counts;  // nb
+  int* bounds;       // 2 nb: each panel's [start, end)
   int* permbuf;
   int* perm;
   int* ptype;
@@ -1052,6 +1054,8 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
     P.st->kstart[(P.panel + 1) & 1] = e;
     P.st->xseq[(P.panel + 1) & 1] = static_cast<int>(seq + 1);  // + the barrier below
     if (P.panel_end) P.panel_end[P.panel] = e;
+    P.bounds[2 * P.panel] = kstart;
+    P.bounds[2 * P.panel + 1] = e;
     if (P.stats) {
       for (int k = 0; k < 5; ++k) atomicAdd(P.stats + k, tm[k]);
       atomicAdd(P.stats + 5, static_cast<unsigned long long>(kb));
@@ -1067,6 +1071,7 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
   }
   // ---- gather the interchanged data (written back by finalize_kernel)
   const int cnt = ldcg(&P.st->moved[P.panel & 1]);
+  if (c == 0 && t == 0) P.move_counts[P.panel] = cnt;
   if (cnt == 0) return;
   const int* list = P.moved + (P.panel & 1) * P.move_cap;
   const long long m = n - kstart;
@@ -1080,11 +1085,14 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
     const int sy = ldcg(P.srcmap + y);
     P.gbuf[ix * ldw + (y - kstart)] = asym(sx, sy);
   }
-  // factored rows q < k0 at the moved columns (their column exchanges, :472-491)
-  for (long long idx = gtid; idx < static_cast<long long>(kstart) * cnt; idx += nthreads) {
-    const int q = static_cast<int>(idx / cnt), ix = static_cast<int>(idx - static_cast<long long>(q) * cnt);
-    const int sx = ldcg(P.srcmap + ldcg(list + ix));
-    P.gbuf2[static_cast<long long>(q) * P.move_cap + ix] = __ldg(P.a + static_cast<long long>(q) * lda + sx);
+  // the moves (position dst receives what position src held): the factored
+  // rows q < k0 take the same column exchanges (:472-491), applied once
+  // after the last panel (launch_left_swaps)
+  int* rec = P.moves + static_cast<size_t>(P.panel) * 2 * P.move_cap;
+  for (long long ix = gtid; ix < cnt; ix += nthreads) {
+    const int x = ldcg(list + ix);
+    rec[ix] = x;
+    rec[P.move_cap + ix] = ldcg(P.srcmap + x);
   }
   for (long long ix = gtid; ix < cnt; ix += nthreads)
     P.permbuf[ix] = ldcg(P.perm + ldcg(P.srcmap + ldcg(list + ix)));
@@ -1093,7 +1101,6 @@ __global__ void __launch_bounds__(kBlock, 1) panel_kernel(PanelArgs P) {
 // Writes back what the panel's interchanges moved, the permutation, and the
 // panel's compact factor rows [k0, e):
 //   A[x, y]  (moved x >= e, y >= e)        from the gathered rows
-//   A[q, x]  (q < k0, moved x)             from the gathered factored rows
 //   perm[x]  (moved x)                     = perm[slot of x] before the panel
 //   A[q, j]  (k0 <= q < e, j >= q)         D entries (dlog) or U[q, j] (ucm)
 struct FinArgs {
@@ -1107,7 +1114,6 @@ struct FinArgs {
   int move_cap;
   const double* gbuf;
   long long ldg;
-  const double* gbuf2;
   const int* permbuf;
   int* perm;
   int n;
@@ -1134,7 +1140,7 @@ __global__ void __launch_bounds__(256) finalize_kernel(FinArgs F) {
   const int* list = F.moved + (F.panel & 1) * F.move_cap;
   if (cnt > 0) {
     // each thread keeps kFinUnroll loads in flight before its stores
-    const long long m = n - e, total1 = cnt * m, total2 = static_cast<long long>(k0) * cnt;
+    const long long m = n - e, total1 = cnt * m;
     for (long long base = gtid; base < total1; base += nthreads * kFinUnroll) {
       double v[kFinUnroll];
       long long dst[kFinUnroll];
@@ -1150,24 +1156,6 @@ __global__ void __launch_bounds__(256) finalize_kernel(FinArgs F) {
             v[u] = F.gbuf[ix * F.ldg + (y - k0)];
             dst[u] = x <= y ? static_cast<long long>(x) * lda + y : static_cast<long long>(y) * lda + x;
           }
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < kFinUnroll; ++u)
-        if (dst[u] >= 0) F.a[dst[u]] = v[u];
-    }
-    for (long long base = gtid; base < total2; base += nthreads * kFinUnroll) {
-      double v[kFinUnroll];
-      long long dst[kFinUnroll];
-#pragma unroll
-      for (int u = 0; u < kFinUnroll; ++u) {
-        const long long idx = base + u * nthreads;
-        dst[u] = -1;
-        v[u] = 0.0;
-        if (idx < total2) {
-          const int q = static_cast<int>(idx / cnt), ix = static_cast<int>(idx - static_cast<long long>(q) * cnt);
-          v[u] = F.gbuf2[static_cast<long long>(q) * F.move_cap + ix];
-          dst[u] = static_cast<long long>(q) * lda + list[ix];
         }
       }
 #pragma unroll
@@ -1206,6 +1194,97 @@ __global__ void __launch_bounds__(256) finalize_kernel(FinArgs F) {
     }
     __syncthreads();
   }
+}
+
+// ---------------------------------------------------------------------------
+// The factored rows' column exchanges, applied once after the last panel.
+// Each panel's interchanges move indices at positions >= its start, and the
+// reference exchanges the same columns of every row factored before, as it
+// goes (:472-491).  Those rows are not read again while the factorization
+// runs, so each panel only records its moves (position dst receives what
+// position src held); from the last panel back, inv maps a position at the
+// end of panel k to its final position, and panel k's rows are scattered in
+// final column order into the gbuf scratch and copied back.  Every entry
+// moves once, by copies coalesced on one side, instead of a scattered read
+// and write per moved column and earlier row at every panel.  pend[parity]
+// counts the moves after panel k: while it is zero the rows stay as they are.
+struct SwapArgs {
+  const int* moves;
+  const int* counts;
+  const int* bounds;
+  int move_cap;
+  int n;
+  int* inv;
+  int* tmp;   // move_cap values, then pend[2]
+  double* a;
+  long long lda;
+  double* scratch;
+  long long lds;
+  const DeviceState* st;
+};
+
+__device__ __forceinline__ void panel_range(const int* bounds, int panel, int n, int& k0, int& e) {
+  k0 = min(max(bounds[2 * panel], 0), n);
+  e = min(max(bounds[2 * panel + 1], k0), n);
+}
+
+// inv_{k-1} = inv_k composed with panel k's moves (inv[src] = inv[dst]); the
+// moves permute the moved positions among themselves.  One CTA.
+__device__ void moves_into_inv(const SwapArgs& S, int panel) {
+  const int cnt = min(max(S.counts[panel], 0), S.move_cap);
+  const int* dst = S.moves + static_cast<size_t>(panel) * 2 * S.move_cap;
+  const int* src = dst + S.move_cap;
+  int* pend = S.tmp + S.move_cap;
+  for (int ix = threadIdx.x; ix < cnt; ix += blockDim.x) {
+    const int d = dst[ix];
+    S.tmp[ix] = d >= 0 && d < S.n ? S.inv[d] : 0;
+  }
+  __syncthreads();
+  for (int ix = threadIdx.x; ix < cnt; ix += blockDim.x) {
+    const int sidx = src[ix];
+    if (sidx >= 0 && sidx < S.n) S.inv[sidx] = S.tmp[ix];
+  }
+  if (threadIdx.x == 0) pend[(panel - 1) & 1] = pend[panel & 1] + cnt;
+}
+
+// inv = identity, pend = 0, then the last panel's moves
+__global__ void swaps_start_kernel(SwapArgs S, int last) {
+  if (ld_relaxed_s32(&S.st->abort)) return;
+  for (int i = threadIdx.x; i < S.n; i += blockDim.x) S.inv[i] = i;
+  if (threadIdx.x == 0) S.tmp[S.move_cap + (last & 1)] = 0;
+  __syncthreads();
+  moves_into_inv(S, last);
+}
+
+// scratch[r][inv[x] - e] = A[k0 + r, x] for panel k's rows
+__global__ void rows_scatter_kernel(SwapArgs S, int panel) {
+  if (ld_relaxed_s32(&S.st->abort) || S.tmp[S.move_cap + (panel & 1)] == 0) return;
+  int k0, e;
+  panel_range(S.bounds, panel, S.n, k0, e);
+  const long long cols = S.n - e, total = static_cast<long long>(e - k0) * cols;
+  for (long long idx = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; idx < total;
+       idx += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int r = static_cast<int>(idx / cols), x = e + static_cast<int>(idx - r * cols);
+    const int f = S.inv[x];
+    if (f >= e && f < S.n) S.scratch[r * S.lds + (f - e)] = S.a[static_cast<long long>(k0 + r) * S.lda + x];
+  }
+}
+
+// A[k0 + r, j] = scratch[r][j - e]; block 0 then folds panel k's moves into
+// inv for panel k - 1 (nothing here reads inv)
+__global__ void rows_back_kernel(SwapArgs S, int panel) {
+  if (ld_relaxed_s32(&S.st->abort)) return;
+  if (S.tmp[S.move_cap + (panel & 1)] != 0) {
+    int k0, e;
+    panel_range(S.bounds, panel, S.n, k0, e);
+    const long long cols = S.n - e, total = static_cast<long long>(e - k0) * cols;
+    for (long long idx = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; idx < total;
+         idx += static_cast<long long>(gridDim.x) * blockDim.x) {
+      const int r = static_cast<int>(idx / cols), j = e + static_cast<int>(idx - r * cols);
+      S.a[static_cast<long long>(k0 + r) * S.lda + j] = S.scratch[r * S.lds + (j - e)];
+    }
+  }
+  if (blockIdx.x == 0 && panel > 0) moves_into_inv(S, panel);
 }
 
 __global__ void init_kernel(int n, int* perm, int* pivot_types, DeviceState* st,
@@ -1315,7 +1394,9 @@ int launch_panel(const FactorPlan& plan, int panel, cudaStream_t s) {
   P.moved = plan.moved;
   P.move_cap = plan.move_cap;
   P.gbuf = plan.gbuf;
-  P.gbuf2 = plan.gbuf2;
+  P.moves = plan.moves;
+  P.move_counts = plan.move_counts;
+  P.bounds = plan.bounds;
   P.permbuf = plan.permbuf;
   P.perm = plan.perm;
   P.ptype = plan.pivot_types;
@@ -1401,6 +1482,23 @@ int launch_wrows(const FactorPlan& plan, int panel, cudaStream_t s) {
   return BBK_OK;
 }
 
+int launch_left_swaps(const FactorPlan& plan, cudaStream_t s) {
+  if (plan.nb < 2) return BBK_OK;
+  const int sms = device_sm_count();
+  SwapArgs S{plan.moves, plan.move_counts, plan.bounds, plan.move_cap, plan.n, plan.posinv, plan.movetmp,
+             plan.a, plan.lda, plan.gbuf, plan.ldw, plan.state};
+  swaps_start_kernel<<<1, 1024, 0, s>>>(S, plan.nb - 1);
+  BBK_CUDA_TRY(cudaGetLastError());
+  count_launch();
+  for (int k = plan.nb - 2; k >= 0; --k) {
+    rows_scatter_kernel<<<4 * sms, 256, 0, s>>>(S, k);
+    rows_back_kernel<<<4 * sms, 256, 0, s>>>(S, k);
+    BBK_CUDA_TRY(cudaGetLastError());
+    count_launch(2);
+  }
+  return BBK_OK;
+}
+
 int launch_finalize(const FactorPlan& plan, int panel, cudaStream_t s) {
   const int sms = device_sm_count();
   FinArgs F{};
@@ -1414,7 +1512,6 @@ int launch_finalize(const FactorPlan& plan, int panel, cudaStream_t s) {
   F.move_cap = plan.move_cap;
   F.gbuf = plan.gbuf;
   F.ldg = plan.ldw;
-  F.gbuf2 = plan.gbuf2;
   F.permbuf = plan.permbuf;
   F.perm = plan.perm;
   F.n = plan.n;
