@@ -468,20 +468,21 @@ __global__ void __launch_bounds__(kThreadsMma) mma_update_kernel(UpdArgs U) {
 // (BN wide) holds row blocks I <= (J + 1) R - 1, R = BN / BM, so the first
 // R J(J+1)/2 tiles are the column blocks before J.
 // ---------------------------------------------------------------------------
-template <int BM, int BN, int WM, int WN, int Stages>
+template <int BM, int BN, int WM, int WN, int Stages, int BK = kBK, int MinBlocks = 1>
 struct Wide {
   static constexpr int kWarps = (BM / WM) * (BN / WN);
   static constexpr int kThreads = kWarps * 32;
+  static constexpr int kMinBlocks = MinBlocks;
   static constexpr int kR = BN / BM;
-  static constexpr int kAPitch = kBK + kPadA;  // A stage [BM][36]: k contiguous
-  static constexpr int kBPitch = BN + kPadB;   // B stage [32][BN + 4]: j contiguous
+  static constexpr int kAPitch = BK + kPadA;  // A stage [BM][BK + 4]: k contiguous
+  static constexpr int kBPitch = BN + kPadB;  // B stage [BK][BN + 4]: j contiguous
   static constexpr int kAStage = BM * kAPitch;
-  static constexpr int kStage = kAStage + kBK * kBPitch;
+  static constexpr int kStage = kAStage + BK * kBPitch;
   static constexpr size_t kBytes = static_cast<size_t>(Stages) * kStage * sizeof(double);
   static constexpr int kMT = WM / 16, kNT = WN / 8;  // m16n8k8 tiles per warp
   static_assert(BN % BM == 0, "column blocks must cover whole row blocks");
   static_assert(kBytes <= 227 * 1024, "stages must fit the shared memory of one CTA");
-  static_assert((BM * kBK / 2) % kThreads == 0 && (kBK * BN / 2) % kThreads == 0, "even copy split");
+  static_assert((BM * BK / 2) % kThreads == 0 && (BK * BN / 2) % kThreads == 0, "even copy split");
 
   __device__ static int tiles(int tn) { return kR * tn * (tn + 1) / 2; }
   __device__ static void origin(const UpdArgs& U, int t, int& i0, int& j0) {
@@ -497,16 +498,16 @@ struct Wide {
     double* bs = st + kAStage;
     const int t = threadIdx.x;
 #pragma unroll
-    for (int u = 0; u < (BM * kBK / 2) / kThreads; ++u) {
+    for (int u = 0; u < (BM * BK / 2) / kThreads; ++u) {
       const int c = t + u * kThreads;
-      const int ii = c / (kBK / 2), kk = (c % (kBK / 2)) * 2;
+      const int ii = c / (BK / 2), kk = (c % (BK / 2)) * 2;
       const int k = k0 + kk;
       const int nvalid = max(0, min(2, U.inner - k));
       const double* src = U.a + static_cast<long long>(i0 + ii) * U.a_si + (nvalid ? k : 0);
       cp_async_16(&as[ii * kAPitch + kk], src, nvalid * 8);
     }
 #pragma unroll
-    for (int u = 0; u < (kBK * BN / 2) / kThreads; ++u) {
+    for (int u = 0; u < (BK * BN / 2) / kThreads; ++u) {
       const int c = t + u * kThreads;
       const int kk = c / (BN / 2), jj = (c % (BN / 2)) * 2;
       const int k = k0 + kk;
@@ -517,10 +518,10 @@ struct Wide {
   }
 };
 
-template <int BM, int BN, int WM, int WN, int Stages>
-__global__ void __launch_bounds__(Wide<BM, BN, WM, WN, Stages>::kThreads)
+template <int BM, int BN, int WM, int WN, int Stages, int BK = kBK, int MinBlocks = 1>
+__global__ void __launch_bounds__(Wide<BM, BN, WM, WN, Stages, BK, MinBlocks>::kThreads, MinBlocks)
     mma_update_wide_kernel(UpdArgs U) {
-  using W = Wide<BM, BN, WM, WN, Stages>;
+  using W = Wide<BM, BN, WM, WN, Stages, BK, MinBlocks>;
   extern __shared__ double smem[];
   if (U.st != nullptr) {
     // panel mode: range from the device state, tiles from the BN-aligned
@@ -537,7 +538,7 @@ __global__ void __launch_bounds__(Wide<BM, BN, WM, WN, Stages>::kThreads)
   const int tn = (U.n - U.tile_i0 + BN - 1) / BN;
   const int ntiles = W::tiles(tn);
   if (static_cast<int>(blockIdx.x) >= ntiles) return;
-  const int nchunks = (U.inner + kBK - 1) / kBK;
+  const int nchunks = (U.inner + BK - 1) / BK;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = lane >> 2, tq = lane & 3;
   const int wm = (warp / (BN / WN)) * WM, wn = (warp % (BN / WN)) * WN;
@@ -550,7 +551,7 @@ __global__ void __launch_bounds__(Wide<BM, BN, WM, WN, Stages>::kThreads)
   W::origin(U, blockIdx.x, ld_i0, ld_j0);
   auto issue = [&]() {
     if (ld_item < items) {
-      W::load(U, smem + static_cast<size_t>(ld_item % Stages) * W::kStage, ld_i0, ld_j0, ld_ch * kBK);
+      W::load(U, smem + static_cast<size_t>(ld_item % Stages) * W::kStage, ld_i0, ld_j0, ld_ch * BK);
       ++ld_item;
       if (++ld_ch == nchunks) {
         ld_ch = 0;
@@ -589,7 +590,7 @@ __global__ void __launch_bounds__(Wide<BM, BN, WM, WN, Stages>::kThreads)
       const double* as = smem + static_cast<size_t>(item % Stages) * W::kStage;
       const double* bs = as + W::kAStage;
 #pragma unroll
-      for (int ks = 0; ks < kBK; ks += 8) {
+      for (int ks = 0; ks < BK; ks += 8) {
         double af[W::kMT][4], bf[W::kNT][2];
 #pragma unroll
         for (int mt = 0; mt < W::kMT; ++mt) {
@@ -646,6 +647,9 @@ __global__ void __launch_bounds__(Wide<BM, BN, WM, WN, Stages>::kThreads)
 // SM so one CTA's barrier waits and epilogue overlap the other's MMAs).
 using WideSquare = Wide<128, 128, 64, 32, 3>;
 using WideHalf = Wide<64, 128, 32, 64, 2>;
+// 64 x 64 tiles, 4 warps of 32 x 32, k chunks of 16 in a 3-stage ring:
+// 56.8 KB of shared memory, so four CTAs (16 warps) per SM
+using WideS3 = Wide<64, 64, 32, 32, 3, 16, 4>;
 
 // ---------------------------------------------------------------------------
 // SIMT tiles: reference-ordered FP64 and FP32.  256 threads, 4x4 per thread.
@@ -740,14 +744,18 @@ bool use_k16() {
 }
 
 // Tile shape of the FP64 tensor-core update for large trailing matrices:
-// BBK_UPDATE_TILE = 64 (64 x 64 everywhere), 128 (128 x 128) or 64x128.
+// by default 64 x 64 tiles in the 3-stage ring of k chunks of 16 (four CTAs
+// per SM; n=40000: 26.9 TFLOP/s against 25.7 for the two-stage 64 x 64
+// kernel).  BBK_UPDATE_TILE (tuning) = 64 (the two-stage 64 x 64 kernel
+// everywhere), 128 (128 x 128), 64x128 or 64s3 (the default).
 int wide_tile_choice() {
   static const int v = [] {
     const char* e = getenv("BBK_UPDATE_TILE");
-    if (!e) return 0;
+    if (!e) return 3;
+    if (std::strcmp(e, "64") == 0) return 0;
     if (std::strcmp(e, "128") == 0) return 1;
     if (std::strcmp(e, "64x128") == 0) return 2;
-    return 0;
+    return 3;
   }();
   return v;
 }
@@ -758,11 +766,11 @@ int wide_tile_choice() {
 int launch_wide(const UpdArgs& U, int choice, long long order, bool* launched, cudaStream_t s) {
   *launched = false;
   const int sms = device_sm_count();
-  const long long tn = (order + 127) / 128;
-  const int per_sm = choice == 1 ? 1 : 2;
-  const long long tiles = (choice == 1 ? 1 : 2) * tn * (tn + 1) / 2;
+  const long long tn = choice == 3 ? (order + 63) / 64 : (order + 127) / 128;
+  const int per_sm = choice == 1 ? 1 : choice == 3 ? 4 : 2;
+  const long long tiles = (choice == 2 ? 2 : 1) * tn * (tn + 1) / 2;
   if (choice == 0 || tiles < 2LL * per_sm * sms) return BBK_OK;
-  static std::once_flag attr_once[2][64];
+  static std::once_flag attr_once[3][64];
   int dev = 0;
   BBK_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64) return set_error(BBK_ERR_NO_DEVICE, "device %d out of range", dev);
@@ -776,7 +784,7 @@ int launch_wide(const UpdArgs& U, int choice, long long order, bool* launched, c
     });
     BBK_CUDA_TRY(attr_err);
     fn<<<grid, WideSquare::kThreads, WideSquare::kBytes, s>>>(U);
-  } else {
+  } else if (choice == 2) {
     auto fn = mma_update_wide_kernel<64, 128, 32, 64, 2>;
     std::call_once(attr_once[1][dev], [&] {
       attr_err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -784,6 +792,14 @@ int launch_wide(const UpdArgs& U, int choice, long long order, bool* launched, c
     });
     BBK_CUDA_TRY(attr_err);
     fn<<<grid, WideHalf::kThreads, WideHalf::kBytes, s>>>(U);
+  } else {
+    auto fn = mma_update_wide_kernel<64, 64, 32, 32, 3, 16, 4>;
+    std::call_once(attr_once[2][dev], [&] {
+      attr_err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(WideS3::kBytes));
+    });
+    BBK_CUDA_TRY(attr_err);
+    fn<<<grid, WideS3::kThreads, WideS3::kBytes, s>>>(U);
   }
   BBK_CUDA_TRY(cudaGetLastError());
   count_launch();
