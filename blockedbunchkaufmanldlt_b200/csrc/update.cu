@@ -647,9 +647,11 @@ __global__ void __launch_bounds__(Wide<BM, BN, WM, WN, Stages, BK, MinBlocks>::k
 // SM so one CTA's barrier waits and epilogue overlap the other's MMAs).
 using WideSquare = Wide<128, 128, 64, 32, 3>;
 using WideHalf = Wide<64, 128, 32, 64, 2>;
-// 64 x 64 tiles, 4 warps of 32 x 32, k chunks of 16 in a 3-stage ring:
-// 56.8 KB of shared memory, so four CTAs (16 warps) per SM
+// 64 x 64 tiles, 4 warps of 32 x 32, k chunks of 16 in a 3-stage ring
+// (56.8 KB of shared memory: four CTAs, 16 warps, per SM) or of 8 in a
+// 4-stage ring (42 KB, 94 registers: five CTAs, 20 warps, per SM)
 using WideS3 = Wide<64, 64, 32, 32, 3, 16, 4>;
+using WideS4 = Wide<64, 64, 32, 32, 4, 8, 5>;
 
 // ---------------------------------------------------------------------------
 // SIMT tiles: reference-ordered FP64 and FP32.  256 threads, 4x4 per thread.
@@ -744,18 +746,20 @@ bool use_k16() {
 }
 
 // Tile shape of the FP64 tensor-core update for large trailing matrices:
-// by default 64 x 64 tiles in the 3-stage ring of k chunks of 16 (four CTAs
-// per SM; n=40000: 26.9 TFLOP/s against 25.7 for the two-stage 64 x 64
-// kernel).  BBK_UPDATE_TILE (tuning) = 64 (the two-stage 64 x 64 kernel
-// everywhere), 128 (128 x 128), 64x128 or 64s3 (the default).
+// by default 64 x 64 tiles in the 4-stage ring of k chunks of 8 (five CTAs
+// per SM; n=40000: 27.9 TFLOP/s, against 26.9 for the 3-stage ring of 16
+// and 25.7 for the two-stage 64 x 64 kernel).  BBK_UPDATE_TILE (tuning) =
+// 64 (the two-stage 64 x 64 kernel everywhere), 128 (128 x 128), 64x128,
+// 64s3 or 64s4 (the default).
 int wide_tile_choice() {
   static const int v = [] {
     const char* e = getenv("BBK_UPDATE_TILE");
-    if (!e) return 3;
+    if (!e) return 4;
     if (std::strcmp(e, "64") == 0) return 0;
     if (std::strcmp(e, "128") == 0) return 1;
     if (std::strcmp(e, "64x128") == 0) return 2;
-    return 3;
+    if (std::strcmp(e, "64s3") == 0) return 3;
+    return 4;
   }();
   return v;
 }
@@ -766,11 +770,11 @@ int wide_tile_choice() {
 int launch_wide(const UpdArgs& U, int choice, long long order, bool* launched, cudaStream_t s) {
   *launched = false;
   const int sms = device_sm_count();
-  const long long tn = choice == 3 ? (order + 63) / 64 : (order + 127) / 128;
-  const int per_sm = choice == 1 ? 1 : choice == 3 ? 4 : 2;
+  const long long tn = choice >= 3 ? (order + 63) / 64 : (order + 127) / 128;
+  const int per_sm = choice == 1 ? 1 : choice == 3 ? 4 : choice == 4 ? 5 : 2;
   const long long tiles = (choice == 2 ? 2 : 1) * tn * (tn + 1) / 2;
   if (choice == 0 || tiles < 2LL * per_sm * sms) return BBK_OK;
-  static std::once_flag attr_once[3][64];
+  static std::once_flag attr_once[4][64];
   int dev = 0;
   BBK_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64) return set_error(BBK_ERR_NO_DEVICE, "device %d out of range", dev);
@@ -792,6 +796,14 @@ int launch_wide(const UpdArgs& U, int choice, long long order, bool* launched, c
     });
     BBK_CUDA_TRY(attr_err);
     fn<<<grid, WideHalf::kThreads, WideHalf::kBytes, s>>>(U);
+  } else if (choice == 4) {
+    auto fn = mma_update_wide_kernel<64, 64, 32, 32, 4, 8, 5>;
+    std::call_once(attr_once[3][dev], [&] {
+      attr_err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(WideS4::kBytes));
+    });
+    BBK_CUDA_TRY(attr_err);
+    fn<<<grid, WideS4::kThreads, WideS4::kBytes, s>>>(U);
   } else {
     auto fn = mma_update_wide_kernel<64, 64, 32, 32, 3, 16, 4>;
     std::call_once(attr_once[2][dev], [&] {
