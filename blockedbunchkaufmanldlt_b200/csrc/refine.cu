@@ -26,9 +26,10 @@ constexpr int kResThreads = 256;
 // R[:, c] = B[:, c] - A X[:, c] for c < nrhs (nrhs <= kMaxRhs), A symmetric
 // stored in its upper triangle (row-major, lda).  One CTA per 64-row block:
 // it streams its row block right of the diagonal and its column block above
-// the diagonal (both as contiguous row segments), so the result is
-// deterministic.  With abs_rowsum != null it also writes sum_j |A(i,j)|.
-__global__ void __launch_bounds__(kResThreads) symm_residual_kernel(
+// the diagonal (both as contiguous row segments), in a fixed order, so the
+// result is deterministic.  With abs_rowsum != null it also writes
+// sum_j |A(i,j)|.
+__global__ void __launch_bounds__(kResThreads, 2) symm_residual_kernel(
     int n, const double* __restrict__ a, long long lda, int nrhs, const double* __restrict__ x,
     long long ldx, const double* __restrict__ b, long long ldb, double* __restrict__ r, long long ldr,
     double* __restrict__ abs_rowsum) {
@@ -36,55 +37,116 @@ __global__ void __launch_bounds__(kResThreads) symm_residual_kernel(
   __shared__ double xs[kRB][kMaxRhs];
   const int i0 = blockIdx.x * kRB;
   const int t = threadIdx.x;
-  // thread -> (row ii, rhs group): 64 rows x 4 groups of 4 rhs
+  // thread -> (row ii, quarter q of each tile's columns): it keeps its 16
+  // entries of a tile in registers and uses each for every right-hand side
+  // (the shared-memory reads per multiply-add were the limit before)
   const int ii = t & (kRB - 1);
-  const int cg = t >> 6;  // 0..3
-  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  const int q = t >> 6;  // 0..3
+  constexpr int kQ = kRB / 4;
+  double acc[kMaxRhs];
+#pragma unroll
+  for (int c = 0; c < kMaxRhs; ++c) acc[c] = 0.0;
   double asum = 0.0;
   const int nblk = (n + kRB - 1) / kRB;
-  for (int bj = 0; bj < nblk; ++bj) {
+  // tile T[ii][jj] = A_sym(i0+ii, j0+jj) and the tile's x rows: loaded into
+  // registers one tile ahead (the next tile's loads are in flight while this
+  // one is multiplied)
+  constexpr int kPer = kRB * kRB / kResThreads;
+  constexpr int kXPer = kRB * kMaxRhs / kResThreads;
+  double v[kPer], xv[kXPer];
+  auto load_tile = [&](int bj) {
     const int j0 = bj * kRB;
-    // tile T[ii][jj] = A_sym(i0+ii, j0+jj)
-    for (int idx = t; idx < kRB * kRB; idx += kResThreads) {
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      const int idx = t + u * kResThreads;
       const int r0 = idx / kRB, c0 = idx % kRB;
-      double v = 0.0;
-      if (bj > blockIdx.x) {  // right of the diagonal block: A(i, j), row segments
+      double x0 = 0.0;
+      if (bj > static_cast<int>(blockIdx.x)) {  // right of the diagonal block: A(i, j), row segments
         const int i = i0 + r0, j = j0 + c0;
-        if (i < n && j < n) v = a[static_cast<long long>(i) * lda + j];
-        at[r0][c0] = v;
+        if (i < n && j < n) x0 = a[static_cast<long long>(i) * lda + j];
       } else if (bj < static_cast<int>(blockIdx.x)) {  // above: A(j, i), row segments of rows j
         const int jrow = j0 + r0, icol = i0 + c0;
-        if (jrow < n && icol < n) v = a[static_cast<long long>(jrow) * lda + icol];
-        at[c0][r0] = v;
+        if (jrow < n && icol < n) x0 = a[static_cast<long long>(jrow) * lda + icol];
       } else {  // diagonal block: mirror the upper triangle
         const int i = i0 + r0, j = j0 + c0;
-        if (i < n && j < n) v = (i <= j) ? a[static_cast<long long>(i) * lda + j] : a[static_cast<long long>(j) * lda + i];
-        at[r0][c0] = v;
+        if (i < n && j < n) x0 = (i <= j) ? a[static_cast<long long>(i) * lda + j] : a[static_cast<long long>(j) * lda + i];
       }
+      v[u] = x0;
     }
-    for (int idx = t; idx < kRB * kMaxRhs; idx += kResThreads) {
+#pragma unroll
+    for (int u = 0; u < kXPer; ++u) {
+      const int idx = t + u * kResThreads;
       const int jj = idx / kMaxRhs, c = idx % kMaxRhs;
       const int j = j0 + jj;
-      xs[jj][c] = (j < n && c < nrhs) ? x[c * ldx + j] : 0.0;
+      xv[u] = (j < n && c < nrhs) ? x[c * ldx + j] : 0.0;
+    }
+  };
+  if (nblk > 0) load_tile(0);
+  for (int bj = 0; bj < nblk; ++bj) {
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      const int idx = t + u * kResThreads;
+      const int r0 = idx / kRB, c0 = idx % kRB;
+      if (bj < static_cast<int>(blockIdx.x))
+        at[c0][r0] = v[u];
+      else
+        at[r0][c0] = v[u];
+    }
+#pragma unroll
+    for (int u = 0; u < kXPer; ++u) {
+      const int idx = t + u * kResThreads;
+      xs[idx / kMaxRhs][idx % kMaxRhs] = xv[u];
     }
     __syncthreads();
-#pragma unroll 8
-    for (int jj = 0; jj < kRB; ++jj) {
-      const double av = at[ii][jj];
-      if (abs_rowsum && cg == 0) asum += fabs(av);
+    if (bj + 1 < nblk) load_tile(bj + 1);
+    double av[kQ];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) acc[u] += av * xs[jj][cg * 4 + u];
+    for (int u = 0; u < kQ; ++u) av[u] = at[ii][q * kQ + u];
+    if (abs_rowsum) {
+#pragma unroll
+      for (int u = 0; u < kQ; ++u) asum += fabs(av[u]);
     }
+#pragma unroll
+    for (int c = 0; c < kMaxRhs; ++c)
+      if (c < nrhs) {
+#pragma unroll
+        for (int u = 0; u < kQ; ++u) acc[c] = __fma_rn(av[u], xs[q * kQ + u][c], acc[c]);
+      }
     __syncthreads();
   }
-  const int i = i0 + ii;
-  if (i < n) {
+  // add the four quarters, (q0 + q2) + (q1 + q3), through the tile buffer
+  // (free: its last readers passed the barrier): quarters 2 and 3 hand over,
+  // then quarter 1
+  double* red = &at[0][0];  // [2][kMaxRhs + 1][kRB]: the sums, then the row sum
+  static_assert(2 * (kMaxRhs + 1) * kRB <= kRB * (kRB + 1), "reduction buffer");
+  auto slot = [&](int h, int c) { return red + (h * (kMaxRhs + 1) + c) * kRB + ii; };
+  if (q >= 2) {
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int c = cg * 4 + u;
-      if (c < nrhs) r[c * ldr + i] = b[c * ldb + i] - acc[u];
-    }
-    if (abs_rowsum && cg == 0) abs_rowsum[i] = asum;
+    for (int c = 0; c < kMaxRhs; ++c)
+      if (c < nrhs) *slot(q - 2, c) = acc[c];
+    *slot(q - 2, kMaxRhs) = asum;
+  }
+  __syncthreads();
+  if (q < 2) {
+#pragma unroll
+    for (int c = 0; c < kMaxRhs; ++c)
+      if (c < nrhs) acc[c] += *slot(q, c);
+    asum += *slot(q, kMaxRhs);
+  }
+  __syncthreads();
+  if (q == 1) {
+#pragma unroll
+    for (int c = 0; c < kMaxRhs; ++c)
+      if (c < nrhs) *slot(0, c) = acc[c];
+    *slot(0, kMaxRhs) = asum;
+  }
+  __syncthreads();
+  const int i = i0 + ii;
+  if (q == 0 && i < n) {
+#pragma unroll
+    for (int c = 0; c < kMaxRhs; ++c)
+      if (c < nrhs) r[c * ldr + i] = b[c * ldb + i] - (acc[c] + *slot(0, c));
+    if (abs_rowsum) abs_rowsum[i] = asum + *slot(0, kMaxRhs);
   }
 }
 
