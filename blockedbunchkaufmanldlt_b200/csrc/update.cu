@@ -1584,13 +1584,26 @@ __global__ void block_scale_kernel(UpdArgs U, double* a_scale, double* b_scale) 
     const bool is_a = blk < nblk;
     const int bi = is_a ? blk : blk - nblk;
     const int c0 = U.tile_i0 + bi * kBM;
+    // consecutive threads walk the operand's contiguous direction (k for
+    // the row-major A block, the column for B), four loads in flight each;
+    // the maximum does not depend on the order
     double m = 0.0;
-    for (int idx = threadIdx.x; idx < kBM * U.inner; idx += blockDim.x) {
-      const int cc = c0 + idx % kBM, k = idx / kBM;
-      if (cc < U.i_lo || cc >= U.n) continue;
-      const double v = is_a ? U.a[static_cast<long long>(cc) * U.a_si + k]
-                            : U.b[static_cast<long long>(k) * U.b_sk + cc];
-      m = fmax(m, fabs(v));
+    const int total = kBM * U.inner;
+    for (int base = threadIdx.x; base < total; base += 4 * blockDim.x) {
+      double v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int idx = base + u * blockDim.x;
+        v[u] = 0.0;
+        if (idx < total) {
+          const int cc = c0 + (is_a ? idx / U.inner : idx % kBM);
+          const int k = is_a ? idx % U.inner : idx / kBM;
+          if (cc >= U.i_lo && cc < U.n)
+            v[u] = is_a ? U.a[static_cast<long long>(cc) * U.a_si + k] : U.b[static_cast<long long>(k) * U.b_sk + cc];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) m = fmax(m, fabs(v[u]));
     }
     for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, off));
     __shared__ double red[8];
