@@ -175,7 +175,10 @@ int bbk_factor_host(int n, int block_size, double* a, long long lda,
  * Solves A X = B for nrhs right-hand sides stored column after column
  * (b[c*ldb + i]); X overwrites B.  A zero 1x1 pivot yields a zero component
  * (the reference zeroes that column of L); a singular 2x2 pivot divides by
- * zero. */
+ * zero.  The triangular sweeps are latency-bound (one dependent step per 64
+ * rows): up to 32 right-hand sides go through them 8 per launch, each CTA
+ * gathering every solved block into its next own block; more go through a
+ * single launch that reads the factor once for all of them. */
 size_t bbk_solve_workspace_size(int n, int nrhs);
 int bbk_solve_device(int n, const double* factors, long long ldf,
                      const int* perm, const int* pivot_types, int nrhs,
